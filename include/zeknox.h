@@ -1,0 +1,152 @@
+/*
+ * zeknox-b200: the C ABI of zeknox's polynomial-commitment path, for one B200.
+ *
+ * Drop-in for the symbols zeknox exports from libzeknox (native/lib.h:21-51,
+ * native/ntt/ntt.h:17-62, native/merkle/merkle.h:21-62): same names, the same
+ * argument layout and meaning, the same RustError convention.  The Rust
+ * (wrappers/rust/src/lib.rs:12-96) and Go (wrappers/go/lib/lib.go:7-212)
+ * bindings link against libzeknox.so / libzeknox.a built from this tree
+ * without change.  Extensions are marked as such.
+ */
+#ifndef ZEKNOX_B200_H
+#define ZEKNOX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define ZK_VISIBLE __attribute__((visibility("default")))
+#else
+#define ZK_VISIBLE
+#endif
+#ifdef __cplusplus
+#define ZK_EXTERN extern "C" ZK_VISIBLE
+#define ZK_BOOL bool
+#else
+#define ZK_EXTERN ZK_VISIBLE
+#define ZK_BOOL char /* C bindings (cgo) see one byte, as native/ntt/ntt.h:11-15 */
+#endif
+
+/* native/utils/rusterror.h:15-41: returned by value; code 0 = success, a
+ * negative cudaError_t for CUDA failures, cudaErrorInvalidValue (1) for bad
+ * arguments.  `message` is malloc'd (strdup) or NULL; the caller frees it. */
+typedef struct RustError {
+    int code;
+    char *message;
+} RustError;
+
+/* native/ntt/ntt.h:17-41 */
+typedef enum { NN, NR, RN, RR } NTT_InputOutputOrder;
+typedef enum { forward, inverse } NTT_Direction;
+typedef enum { standard, coset } NTT_Type;
+typedef enum { GS, CT } NTT_Algorithm;
+
+/* native/ntt/ntt.h:43-54 (24 bytes).  `order`, `ntt_type` and `is_multi_gpu`
+ * are not read by the single-GPU path, as in zeknox. */
+typedef struct {
+    uint32_t batches;
+    NTT_InputOutputOrder order;
+    NTT_Type ntt_type;
+    uint32_t extension_rate_bits;
+    ZK_BOOL are_inputs_on_device;
+    ZK_BOOL are_outputs_on_device;
+    ZK_BOOL with_coset;
+    ZK_BOOL is_multi_gpu;
+    uint32_t salt_size;
+} NTT_Config;
+
+/* native/ntt/ntt.h:56-61 (8 bytes). */
+typedef struct {
+    uint32_t batches;
+    ZK_BOOL are_inputs_on_device;
+    ZK_BOOL are_outputs_on_device;
+} NTT_TransposeConfig;
+
+/* native/merkle/merkle.h:21-28 */
+enum HashType { HashPoseidon = 0, HashKeccak = 1, HashPoseidonBN128 = 2, HashPoseidon2 = 3, HashMonolith = 4 };
+
+#ifndef HASH_SIZE_U64
+#define HASH_SIZE_U64 4
+#endif
+
+/* ---- device queries (native/lib.h:21-23; bodies native/lib.cu:36-70) ---- */
+ZK_EXTERN RustError get_number_of_gpus(size_t *ngpus);
+ZK_EXTERN RustError list_devices_info(void);
+
+/* ---- table set-up (native/lib.h:25-31; native/lib.cu:115-175) ----
+ * init_cuda() = init_cuda_degree(24); init_cuda_degree(d) =
+ * init_cuda_degree_and_generator(d, 7): the coset table for 2^d points and the
+ * twiddles for every size 2^2..2^d, on every GPU.  Tables are also built on
+ * first use, so these calls are optional warm-ups here. */
+ZK_EXTERN void init_cuda(void);
+ZK_EXTERN void init_cuda_degree(const uint32_t max_degree);
+ZK_EXTERN void init_cuda_degree_and_generator(const uint32_t max_degree, const uint64_t group_generator);
+ZK_EXTERN RustError init_twiddle_factors(size_t device_id, size_t lg_n);
+ZK_EXTERN RustError init_coset(size_t device_id, size_t lg_domain_size, const uint64_t coset_gen);
+
+/* ---- NTT / LDE / transpose (native/lib.h:33-51; native/ntt/ntt.cu:182-564) ----
+ * All synchronous.  Host buffers are staged through device memory owned by the
+ * library.  Sizes: compute_batched_ntt works in place on batches * 2^lg
+ * elements; compute_batched_lde reads batches * 2^lg_n and writes
+ * (batches + salt_size) * 2^(lg_n + extension_rate_bits); transpose reads
+ * batches * 2^lg_n and writes 2^lg_n rows of `batches` elements. */
+ZK_EXTERN RustError compute_batched_ntt(size_t device_id, void *inout, uint32_t lg_domain_size,
+                                        NTT_Direction ntt_direction, NTT_Config cfg);
+ZK_EXTERN RustError compute_batched_lde(size_t device_id, void *output, void *input, uint32_t lg_domain_size,
+                                        NTT_Direction ntt_direction, NTT_Config cfg);
+ZK_EXTERN RustError compute_batched_lde_multi_gpu(void *output, void *input, uint32_t num_gpu,
+                                                  NTT_Direction ntt_direction, NTT_Config cfg,
+                                                  uint32_t lg_domain_size, size_t total_num_input_elements,
+                                                  size_t total_num_output_elements);
+ZK_EXTERN RustError compute_transpose_rev(size_t device_id, void *output, void *input, uint32_t lg_n,
+                                          NTT_TransposeConfig cfg);
+/* Declared by native/lib.h:50 but defined nowhere in zeknox; here an alias of
+ * compute_transpose_rev. */
+ZK_EXTERN RustError compute_naive_transpose_rev(size_t device_id, void *output, void *input, uint32_t lg_n,
+                                                NTT_TransposeConfig cfg);
+
+/* ---- Merkle (native/merkle/merkle.h:30-62; native/merkle/merkle.cu:246-280) ----
+ * Linear digest layout: 2^cap_height subtrees, subtree s owns digests
+ * [s*D, (s+1)*D) with D = digests_buf_size >> cap_height; leaf j of a subtree
+ * sits at D - L + j (L = leaves per subtree); node i's children are 2(i+1) and
+ * 2(i+1)+1; cap[s] = H(node 0, node 1).  Sizes count 4-element digests and
+ * leaves.  The GPU variant takes device pointers, enqueues on the legacy
+ * default stream and returns without synchronising (as zeknox does); gpu_id
+ * is ignored and the current device is used.  Unsupported hash types return
+ * without writing.  fill_digests_buf_linear_cpu takes host pointers and runs
+ * the same kernels through staging buffers (synchronous). */
+ZK_EXTERN void fill_digests_buf_linear_gpu_with_gpu_ptr(void *digests_buf_gpu_ptr, void *cap_buf_gpu_ptr,
+                                                        void *leaves_buf_gpu_ptr, uint64_t digests_buf_size,
+                                                        uint64_t cap_buf_size, uint64_t leaves_buf_size,
+                                                        uint64_t leaf_size, uint64_t cap_height,
+                                                        uint64_t hash_type, uint64_t gpu_id);
+ZK_EXTERN void fill_digests_buf_linear_multigpu_with_gpu_ptr(void *digests_buf_gpu_ptr, void *cap_buf_gpu_ptr,
+                                                             void *leaves_buf_gpu_ptr, uint64_t digests_buf_size,
+                                                             uint64_t cap_buf_size, uint64_t leaves_buf_size,
+                                                             uint64_t leaf_size, uint64_t cap_height,
+                                                             uint64_t hash_type);
+ZK_EXTERN void fill_digests_buf_linear_cpu(void *digests_buf_ptr, void *cap_buf_ptr, const void *leaves_buf_ptr,
+                                           uint64_t digests_buf_size, uint64_t cap_buf_size,
+                                           uint64_t leaves_buf_size, uint64_t leaf_size, uint64_t cap_height,
+                                           uint64_t hash_type);
+
+/* ================= extensions (no counterpart in zeknox) ================= */
+
+/* Last error recorded by a void entry point on this thread (0 = none), e.g.
+ * invalid Merkle sizes; cleared when read. */
+ZK_EXTERN RustError zk_last_error(void);
+
+/* Number of kernels this library has launched in this process. */
+ZK_EXTERN uint64_t zk_kernel_launches(void);
+
+/* Stream-ordered variants for callers that manage their own CUDA streams
+ * (device pointers only, no synchronisation; `stream` is a cudaStream_t). */
+ZK_EXTERN RustError zk_lde_async(void *d_output, const void *d_input, uint32_t lg_n, uint32_t rate_bits,
+                                 uint32_t batches, uint32_t inv, uint32_t with_coset, void *stream);
+ZK_EXTERN RustError zk_transpose_rev_async(void *d_output, const void *d_input, uint32_t lg_n, uint32_t batches,
+                                           void *stream);
+ZK_EXTERN RustError zk_merkle_async(void *d_digests, void *d_cap, const void *d_leaves, uint64_t n_digests,
+                                    uint64_t n_caps, uint64_t n_leaves, uint64_t leaf_size, uint64_t cap_height,
+                                    uint64_t hash_type, void *stream);
+
+#endif /* ZEKNOX_B200_H */

@@ -1,0 +1,389 @@
+/*
+ * ORACLE -- test infrastructure only.
+ *
+ * A plain-C, single-purpose restatement of zeknox's polynomial-commitment
+ * path, used as the checker for the CUDA library: tests, smoke() and the
+ * bench's cpu_baseline leg call it; nothing in the product links it.
+ *
+ * Parity is pinned (tests/test_oracle.py) against
+ *   - the known-answer vectors of zeknox's own tests (native/tests/tests.cu
+ *     Poseidon :279-292, Poseidon2 :409-428, Keccak :164-173; Go Merkle caps
+ *     wrappers/go/lib/lib_test.go:194-213), committed in tests/golden/, and
+ *   - outputs of zeknox's own C++ CPU Merkle path compiled from its sources
+ *     (oracle/build_ref.sh -> oracle/_ref/), committed as fixtures.
+ *
+ * Every routine cites the zeknox file:line whose behaviour it restates.
+ * Field elements are u64, canonical in [0, p), p = 2^64 - 2^32 + 1.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ZK_CONST_TABLE static const
+#include "../zeknox_b200/csrc/zk_constants.h"
+
+typedef uint64_t u64;
+typedef unsigned __int128 u128;
+
+static const u64 P = 0xffffffff00000001ull;
+
+/* ------------------------------------------------------------------ field */
+/* ff/goldilocks.hpp:139-177 (cpp_gl64_t modulo_add / modulo_sub / reduce128),
+ * restated as plain modular arithmetic with canonical results. */
+/* x mod p for any 128-bit x, using 2^64 = 2^32 - 1 and 2^96 = -1 (mod p):
+ * x = lo + 2^64 (h0 + 2^32 h1) = lo + h0 (2^32 - 1) - h1; the sum below is
+ * < 3 * 2^64 and positive, so a few subtractions finish the reduction. */
+static u64 red128(u128 x) {
+    u64 lo = (u64)x, hi = (u64)(x >> 64);
+    u128 r = (u128)lo + (u128)(hi & 0xffffffffull) * 0xffffffffull + P - (hi >> 32);
+    while (r >= P) r -= P;
+    return (u64)r;
+}
+u64 orc_add(u64 a, u64 b) { return red128((u128)a + b); }
+u64 orc_sub(u64 a, u64 b) { return red128((u128)a + P - (b % P)); }
+u64 orc_mul(u64 a, u64 b) { return red128((u128)a * b); }
+u64 orc_pow(u64 a, u64 e) {
+    u64 r = 1;
+    a = red128(a);
+    while (e) {
+        if (e & 1) r = orc_mul(r, a);
+        a = orc_mul(a, a);
+        e >>= 1;
+    }
+    return r;
+}
+u64 orc_inv(u64 a) { return orc_pow(a, P - 2); }
+
+/* ff/gl64_params.hpp:12-87: GROUP_GENERATOR = 7; OMEGA[k] is a primitive
+ * 2^k-th root of unity, OMEGA[k] = 7^((p-1)/2^k) (scripts/gen_field_params.py
+ * squares the 2^32-nd root down); OMEGA_INV[k] its inverse; DOMAIN_SIZE_INV[k]
+ * = 2^-k. */
+u64 orc_omega(unsigned lg) { return orc_pow(7, (P - 1) >> lg); }
+u64 orc_omega_inv(unsigned lg) { return orc_inv(orc_omega(lg)); }
+u64 orc_domain_size_inv(unsigned lg) { return orc_inv(orc_pow(2, lg)); }
+
+/* --------------------------------------------------------------- Poseidon */
+/* poseidon/poseidon.cu:602-791 (the naive permutation the GPU path runs):
+ * 4 full rounds, 22 partial rounds, 4 full rounds; each round adds 12 round
+ * constants, applies x^7 (all lanes / lane 0), then the MDS layer
+ * out[r] = sum_i circ[i] * x[(i + r) % 12] + diag[r] * x[r]. */
+static u64 sbox7(u64 x) {
+    u64 x2 = orc_mul(x, x), x4 = orc_mul(x2, x2), x3 = orc_mul(x, x2);
+    return orc_mul(x3, x4);
+}
+static void poseidon_mds(u64 st[12]) {
+    u64 out[12];
+    for (int r = 0; r < 12; r++) {
+        u128 acc = 0;
+        for (int i = 0; i < 12; i++) acc += (u128)st[(i + r) % 12] * ZK_POSEIDON_MDS_CIRC[i];
+        acc += (u128)st[r] * ZK_POSEIDON_MDS_DIAG[r];
+        out[r] = red128(acc);
+    }
+    memcpy(st, out, sizeof(out));
+}
+void orc_poseidon_permute(u64 st[12]) {
+    int rnd = 0;
+    for (int k = 0; k < 4; k++, rnd++) {
+        for (int i = 0; i < 12; i++) st[i] = sbox7(orc_add(st[i], ZK_POSEIDON_RC[12 * rnd + i]));
+        poseidon_mds(st);
+    }
+    for (int k = 0; k < 22; k++, rnd++) {
+        for (int i = 0; i < 12; i++) st[i] = orc_add(st[i], ZK_POSEIDON_RC[12 * rnd + i]);
+        st[0] = sbox7(st[0]);
+        poseidon_mds(st);
+    }
+    for (int k = 0; k < 4; k++, rnd++) {
+        for (int i = 0; i < 12; i++) st[i] = sbox7(orc_add(st[i], ZK_POSEIDON_RC[12 * rnd + i]));
+        poseidon_mds(st);
+    }
+}
+
+/* -------------------------------------------------------------- Poseidon2 */
+/* poseidon2/poseidon2.cu:61-209: initial external layer, 4 external rounds
+ * (RC, x^7 on all lanes, external layer), 22 internal rounds (RC on lane 0,
+ * x^7 on lane 0, x_i <- x_i * D_i + sum), 4 external rounds.  The external
+ * layer applies the 4x4 block [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]]
+ * (apply_m_4, poseidon2.cu:64-78) to each quarter and adds the column sums. */
+static void p2_m4(u64 *x) {
+    static const int M[4][4] = {{5, 7, 1, 3}, {4, 6, 1, 1}, {1, 3, 5, 7}, {1, 1, 4, 6}};
+    u64 o[4];
+    for (int r = 0; r < 4; r++) {
+        u128 acc = 0;
+        for (int c = 0; c < 4; c++) acc += (u128)x[c] * M[r][c];
+        o[r] = red128(acc);
+    }
+    memcpy(x, o, sizeof(o));
+}
+static void p2_external(u64 st[12]) {
+    for (int i = 0; i < 12; i += 4) p2_m4(st + i);
+    u64 s[4];
+    for (int j = 0; j < 4; j++) s[j] = orc_add(orc_add(st[j], st[j + 4]), st[j + 8]);
+    for (int i = 0; i < 12; i++) st[i] = orc_add(st[i], s[i % 4]);
+}
+void orc_poseidon2_permute(u64 st[12]) {
+    p2_external(st);
+    for (int r = 0; r < 4; r++) {
+        for (int i = 0; i < 12; i++) st[i] = sbox7(orc_add(st[i], ZK_POSEIDON2_RC[12 * r + i]));
+        p2_external(st);
+    }
+    for (int r = 4; r < 26; r++) {
+        st[0] = sbox7(orc_add(st[0], ZK_POSEIDON2_RC[12 * r]));
+        u64 sum = 0;
+        for (int i = 0; i < 12; i++) sum = orc_add(sum, st[i]);
+        for (int i = 0; i < 12; i++) st[i] = orc_add(orc_mul(st[i], ZK_POSEIDON2_DIAG[i]), sum);
+    }
+    for (int r = 26; r < 30; r++) {
+        for (int i = 0; i < 12; i++) st[i] = sbox7(orc_add(st[i], ZK_POSEIDON2_RC[12 * r + i]));
+        p2_external(st);
+    }
+}
+
+/* ----------------------------------------------------------------- Keccak */
+/* keccak/keccak.cu:42-112: Keccak-f[1600], 24 rounds; sponge with rate
+ * 200 - 2*32 = 136 bytes, pad byte 0x01 after the message and 0x80 into the
+ * last rate byte; output the first 32 bytes of the state (little-endian). */
+static u64 rotl(u64 x, int s) { return s ? (x << s) | (x >> (64 - s)) : x; }
+static void keccak_f(u64 a[25]) {
+    for (int rnd = 0; rnd < 24; rnd++) {
+        u64 c[5], d[5], b[25];
+        for (int x = 0; x < 5; x++) c[x] = a[x] ^ a[x + 5] ^ a[x + 10] ^ a[x + 15] ^ a[x + 20];
+        for (int x = 0; x < 5; x++) d[x] = c[(x + 4) % 5] ^ rotl(c[(x + 1) % 5], 1);
+        for (int i = 0; i < 25; i++) a[i] ^= d[i % 5];
+        /* rho + pi: B[y, 2x+3y] = rot(A[x, y], r[x, y]) */
+        for (int x = 0; x < 5; x++)
+            for (int y = 0; y < 5; y++) b[y + 5 * ((2 * x + 3 * y) % 5)] = rotl(a[x + 5 * y], ZK_KECCAK_RHO[x + 5 * y]);
+        for (int y = 0; y < 5; y++)
+            for (int x = 0; x < 5; x++)
+                a[x + 5 * y] = b[x + 5 * y] ^ (~b[(x + 1) % 5 + 5 * y] & b[(x + 2) % 5 + 5 * y]);
+        a[0] ^= ZK_KECCAK_RC[rnd];
+    }
+}
+void orc_keccak256(const uint8_t *in, size_t len, uint8_t out[32]) {
+    u64 st[25] = {0};
+    const size_t rate = 136;
+    uint8_t blk[136];
+    while (len >= rate) {
+        for (int i = 0; i < 17; i++) {
+            u64 w;
+            memcpy(&w, in + 8 * i, 8);
+            st[i] ^= w;
+        }
+        keccak_f(st);
+        in += rate;
+        len -= rate;
+    }
+    memset(blk, 0, rate);
+    memcpy(blk, in, len);
+    blk[len] = 0x01;
+    blk[rate - 1] |= 0x80;
+    for (int i = 0; i < 17; i++) {
+        u64 w;
+        memcpy(&w, blk + 8 * i, 8);
+        st[i] ^= w;
+    }
+    keccak_f(st);
+    memcpy(out, st, 32);
+}
+
+/* ---------------------------------------------------------------- hashers */
+enum { H_POSEIDON = 0, H_KECCAK = 1, H_POSEIDON2 = 3 };
+
+/* Sponge of poseidon/poseidon_permutation.cuh:226-276 (GPU) and
+ * poseidon_permutation.hpp:84-139 (CPU): width 12, rate 8, overwrite mode.
+ * n <= 4: copy and zero-pad (no permutation).  Otherwise for each 8-element
+ * chunk overwrite lanes 0..len-1 (a short final chunk leaves the other lanes
+ * as they are) and permute; the digest is lanes 0..3. */
+static void sponge_hash_one(void (*perm)(u64 *), const u64 *in, u64 n, u64 out[4]) {
+    if (n <= 4) {
+        u64 i = 0;
+        for (; i < n; i++) out[i] = in[i];
+        for (; i < 4; i++) out[i] = 0;
+        return;
+    }
+    u64 st[12] = {0};
+    for (u64 idx = 0; idx < n; idx += 8) {
+        u64 len = n - idx < 8 ? n - idx : 8;
+        for (u64 j = 0; j < len; j++) st[j] = in[idx + j];
+        perm(st);
+    }
+    memcpy(out, st, 32);
+}
+static void sponge_hash_two(void (*perm)(u64 *), const u64 *l, const u64 *r, u64 out[4]) {
+    u64 st[12] = {0};
+    memcpy(st, l, 32);
+    memcpy(st + 4, r, 32);
+    perm(st);
+    memcpy(out, st, 32);
+}
+/* keccak/keccak.cu:116-135: n < 4 copies n words and leaves the rest of the
+ * digest untouched; otherwise keccak256 over the 8n little-endian bytes,
+ * then digest[3] &= 0xff.  hash_two hashes left[0..25) || right[0..25). */
+static void keccak_hash_one(const u64 *in, u64 n, u64 out[4]) {
+    if (n < 4) {
+        memcpy(out, in, n * 8);
+        return;
+    }
+    orc_keccak256((const uint8_t *)in, n * 8, (uint8_t *)out);
+    out[3] &= 0xff;
+}
+static void keccak_hash_two(const u64 *l, const u64 *r, u64 out[4]) {
+    uint8_t buf[50];
+    memcpy(buf, l, 25);
+    memcpy(buf + 25, r, 25);
+    orc_keccak256(buf, 50, (uint8_t *)out);
+    out[3] &= 0xff;
+}
+
+int orc_hash_one(int ht, const u64 *in, u64 n, u64 out[4]) {
+    switch (ht) {
+    case H_POSEIDON: sponge_hash_one(orc_poseidon_permute, in, n, out); return 0;
+    case H_POSEIDON2: sponge_hash_one(orc_poseidon2_permute, in, n, out); return 0;
+    case H_KECCAK: keccak_hash_one(in, n, out); return 0;
+    default: return -1;
+    }
+}
+int orc_hash_two(int ht, const u64 *l, const u64 *r, u64 out[4]) {
+    switch (ht) {
+    case H_POSEIDON: sponge_hash_two(orc_poseidon_permute, l, r, out); return 0;
+    case H_POSEIDON2: sponge_hash_two(orc_poseidon2_permute, l, r, out); return 0;
+    case H_KECCAK: keccak_hash_two(l, r, out); return 0;
+    default: return -1;
+    }
+}
+
+/* ----------------------------------------------------------------- Merkle */
+/* merkle/merkle.cu:166-244 (the GPU driver the C ABI runs):
+ *  - n_caps == n_leaves: cap[i] = H1(leaf i); digests untouched.
+ *  - subtree of L_s = n_leaves >> cap_height leaves, D_s = n_digests >> cap_height
+ *    digests; L_s == 1: cap[i] = H1(leaf i).  L_s == 2: digest[i] = H1(leaf i),
+ *    cap[s] = H2(digest[s D_s], digest[s D_s + 1]).
+ *  - general: subtree s, leaf j -> digest s D_s + (D_s - L_s) + j; internal
+ *    node i of subtree s (linear index inside the subtree) has children
+ *    2(i+1), 2(i+1)+1; level widths 2^r at offsets 2^r - 2; cap[s] =
+ *    H2(node 0, node 1). */
+int orc_merkle_fill(u64 *digests, u64 *cap, const u64 *leaves, u64 n_digests, u64 n_caps,
+                    u64 n_leaves, u64 leaf_size, u64 cap_height, int ht) {
+    if (ht != H_POSEIDON && ht != H_POSEIDON2 && ht != H_KECCAK) return -1;
+    if (n_caps == n_leaves) {
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < (long long)n_leaves; i++)
+            orc_hash_one(ht, leaves + i * leaf_size, leaf_size, cap + 4 * i);
+        return 0;
+    }
+    u64 Ds = n_digests >> cap_height, Ls = n_leaves >> cap_height;
+    if (Ls == 1) {
+        for (u64 i = 0; i < n_leaves; i++) orc_hash_one(ht, leaves + i * leaf_size, leaf_size, cap + 4 * i);
+        return 0;
+    }
+    if (Ls == 2) {
+        for (u64 i = 0; i < n_leaves; i++) orc_hash_one(ht, leaves + i * leaf_size, leaf_size, digests + 4 * i);
+        for (u64 s = 0; s < n_caps; s++) orc_hash_two(ht, digests + 4 * s * Ds, digests + 4 * (s * Ds + 1), cap + 4 * s);
+        return 0;
+    }
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)n_leaves; i++) {
+        u64 s = i / Ls, j = i % Ls;
+        orc_hash_one(ht, leaves + i * leaf_size, leaf_size, digests + 4 * (s * Ds + (Ds - Ls) + j));
+    }
+    for (u64 w = Ls / 2; w >= 2; w /= 2) {
+        u64 off = w - 2;
+#pragma omp parallel for schedule(static)
+        for (long long t = 0; t < (long long)(w * n_caps); t++) {
+            u64 s = t / w, i = off + t % w;
+            u64 *base = digests + 4 * s * Ds;
+            orc_hash_two(ht, base + 4 * (2 * (i + 1)), base + 4 * (2 * (i + 1) + 1), base + 4 * i);
+        }
+    }
+    for (u64 s = 0; s < n_caps; s++) orc_hash_two(ht, digests + 4 * s * Ds, digests + 4 * (s * Ds + 1), cap + 4 * s);
+    return 0;
+}
+
+/* -------------------------------------------------------------------- NTT */
+static u64 bitrev(u64 x, unsigned bits) {
+    u64 r = 0;
+    for (unsigned i = 0; i < bits; i++) r |= ((x >> i) & 1) << (bits - 1 - i);
+    return r;
+}
+/* Plain transform X[k] = sum_i a[i] w^(ik), w = OMEGA[lg] (forward) or
+ * OMEGA_INV[lg] (inverse), natural order in and out, no scaling.  Computed
+ * by bit-reversal + iterative radix-2 Cooley-Tukey. */
+void orc_ntt_raw(u64 *a, unsigned lg, int inverse) {
+    u64 n = 1ull << lg;
+    for (u64 i = 0; i < n; i++) {
+        u64 j = bitrev(i, lg);
+        if (i < j) {
+            u64 t = a[i];
+            a[i] = a[j];
+            a[j] = t;
+        }
+    }
+    for (unsigned s = 1; s <= lg; s++) {
+        u64 m = 1ull << s, h = m >> 1;
+        u64 wm = inverse ? orc_omega_inv(s) : orc_omega(s);
+        u64 *tw = (u64 *)malloc(h * sizeof(u64));
+        tw[0] = 1;
+        for (u64 j = 1; j < h; j++) tw[j] = orc_mul(tw[j - 1], wm);
+        for (u64 k = 0; k < n; k += m)
+            for (u64 j = 0; j < h; j++) {
+                u64 u = a[k + j], v = orc_mul(a[k + j + h], tw[j]);
+                a[k + j] = orc_add(u, v);
+                a[k + j + h] = orc_sub(u, v);
+            }
+        free(tw);
+    }
+}
+
+/* ntt/ntt.cu:106-158 + :253-309 (batch_ntt):
+ *  forward: [x_i *= coset_i if with_coset]; X = NTT_w(x), natural order.
+ *  inverse: y = NTT_{w^-1}(x) natural order; [y_i *= coset_i if with_coset];
+ *           y_i *= 2^-lg.
+ * coset_i = coset_gen^i (the table init_coset writes, ntt.cu:228-239). */
+void orc_batch_ntt(u64 *inout, unsigned lg, int inverse, unsigned batches, int with_coset, u64 coset_gen) {
+    u64 n = 1ull << lg;
+#pragma omp parallel for schedule(dynamic)
+    for (long long b = 0; b < (long long)batches; b++) {
+        u64 *a = inout + b * n;
+        if (!inverse) {
+            if (with_coset) {
+                u64 g = 1;
+                for (u64 i = 0; i < n; i++, g = orc_mul(g, coset_gen)) a[i] = orc_mul(a[i], g);
+            }
+            orc_ntt_raw(a, lg, 0);
+        } else {
+            orc_ntt_raw(a, lg, 1);
+            u64 ninv = orc_domain_size_inv(lg);
+            u64 g = 1;
+            for (u64 i = 0; i < n; i++) {
+                if (with_coset) {
+                    a[i] = orc_mul(a[i], g);
+                    g = orc_mul(g, coset_gen);
+                }
+                a[i] = orc_mul(a[i], ninv);
+            }
+        }
+    }
+}
+
+/* ntt/ntt.cu:477-564 (batch_lde): zero-extend each of the `batches` rows from
+ * 2^lg_n to N = 2^(lg_n + rate_bits) elements (kernels.cu:40-60), then the
+ * size-N batch_ntt above on the extended rows. */
+void orc_batch_lde(u64 *out, const u64 *in, unsigned lg_n, unsigned rate_bits, int inverse, unsigned batches,
+                   int with_coset, u64 coset_gen) {
+    u64 n = 1ull << lg_n, N = n << rate_bits;
+    for (u64 b = 0; b < batches; b++) {
+        memcpy(out + b * N, in + b * n, n * sizeof(u64));
+        memset(out + b * N + n, 0, (N - n) * sizeof(u64));
+    }
+    orc_batch_ntt(out, lg_n + rate_bits, inverse, batches, with_coset, coset_gen);
+}
+
+/* ntt/kernels.cu:94-135 (transpose_rev_kernel): out[rev_lg(k)][b] = in[b][k]
+ * for b < batches, k < 2^lg_n (equivalently out[k][b] = in[b][rev(k)]). */
+void orc_transpose_rev(u64 *out, const u64 *in, unsigned lg_n, unsigned batches) {
+    u64 n = 1ull << lg_n;
+#pragma omp parallel for schedule(static)
+    for (long long k = 0; k < (long long)n; k++) {
+        u64 r = bitrev(k, lg_n);
+        for (u64 b = 0; b < batches; b++) out[r * batches + b] = in[b * n + k];
+    }
+}

@@ -1,0 +1,206 @@
+"""ORACLE -- test infrastructure only.
+
+ctypes front end of ``liboracle.so`` (the C restatement in oracle.c) and of
+zeknox's own CPU build in ``_ref/libzkref_cpu.so`` (built by build_ref.sh when
+the zeknox sources are present).  Only tests/, ``__graft_entry__.smoke()`` and
+the bench's cpu_baseline / reference legs import this module, and only as the
+checker or the timed CPU baseline: the product never routes through it.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_LIB = None
+_REF = None
+
+HASH_POSEIDON, HASH_KECCAK, HASH_POSEIDON_BN128, HASH_POSEIDON2, HASH_MONOLITH = 0, 1, 2, 3, 4
+P = 0xFFFFFFFF00000001
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_u64p)
+
+
+def build() -> Path:
+    """Compile liboracle.so (plain C, gcc) if it is missing or stale."""
+    so = HERE / "liboracle.so"
+    src = [HERE / "oracle.c", HERE.parent / "zeknox_b200" / "csrc" / "zk_constants.h"]
+    if not so.exists() or any(s.stat().st_mtime > so.stat().st_mtime for s in src):
+        subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
+    return so
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = ctypes.CDLL(str(build()))
+        L = _LIB
+        u64, u32, c_int, vp = ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p
+        for name in ("orc_add", "orc_sub", "orc_mul", "orc_pow"):
+            getattr(L, name).argtypes = [u64, u64]
+            getattr(L, name).restype = u64
+        for name in ("orc_omega", "orc_omega_inv", "orc_domain_size_inv"):
+            getattr(L, name).argtypes = [ctypes.c_uint]
+            getattr(L, name).restype = u64
+        L.orc_poseidon_permute.argtypes = [_u64p]
+        L.orc_poseidon2_permute.argtypes = [_u64p]
+        L.orc_keccak256.argtypes = [vp, ctypes.c_size_t, vp]
+        L.orc_hash_one.argtypes = [c_int, _u64p, u64, _u64p]
+        L.orc_hash_one.restype = c_int
+        L.orc_hash_two.argtypes = [c_int, _u64p, _u64p, _u64p]
+        L.orc_hash_two.restype = c_int
+        L.orc_merkle_fill.argtypes = [_u64p, _u64p, _u64p, u64, u64, u64, u64, u64, c_int]
+        L.orc_merkle_fill.restype = c_int
+        L.orc_ntt_raw.argtypes = [_u64p, ctypes.c_uint, c_int]
+        L.orc_batch_ntt.argtypes = [_u64p, ctypes.c_uint, c_int, ctypes.c_uint, c_int, u64]
+        L.orc_batch_lde.argtypes = [_u64p, _u64p, ctypes.c_uint, ctypes.c_uint, c_int, ctypes.c_uint, c_int, u64]
+        L.orc_transpose_rev.argtypes = [_u64p, _u64p, ctypes.c_uint, ctypes.c_uint]
+    return _LIB
+
+
+def ref_available() -> bool:
+    return (HERE / "_ref" / "libzkref_cpu.so").exists()
+
+
+def ref():
+    """zeknox's own CPU path (compiled from its sources), or None if not built."""
+    global _REF
+    if _REF is None and ref_available():
+        _REF = ctypes.CDLL(str(HERE / "_ref" / "libzkref_cpu.so"))
+        u64, vp = ctypes.c_uint64, ctypes.c_void_p
+        _REF.fill_digests_buf_linear_cpu.argtypes = [vp, vp, vp, u64, u64, u64, u64, u64, u64]
+        _REF.fill_digests_buf_linear_cpu.restype = None
+        _REF.zkref_hash_one.argtypes = [ctypes.c_int, _u64p, u64, _u64p]
+        _REF.zkref_hash_two.argtypes = [ctypes.c_int, _u64p, _u64p, _u64p]
+    return _REF
+
+
+# ---------------------------------------------------------------- data
+def splitmix64(seed: int, n: int) -> np.ndarray:
+    """SplitMix64 stream (Steele, Lea, Flood 2014), vectorised."""
+    idx = np.arange(1, n + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + idx * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return z
+
+
+def field_elems(seed: int, n: int) -> np.ndarray:
+    """n uniform canonical field elements: SplitMix64 words rejection-sampled to [0, p)."""
+    out = np.empty(0, dtype=np.uint64)
+    s = seed
+    while out.size < n:
+        z = splitmix64(s, n - out.size + 64)
+        out = np.concatenate([out, z[z < np.uint64(P)]])
+        s = (s * 0x9E3779B97F4A7C15 + 1) & 0xFFFFFFFFFFFFFFFF
+    return np.ascontiguousarray(out[:n])
+
+
+# ---------------------------------------------------------------- hashing
+def hash_one(ht: int, leaf: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+    leaf = np.ascontiguousarray(leaf, dtype=np.uint64)
+    out = np.zeros(4, dtype=np.uint64) if out is None else out
+    if lib().orc_hash_one(ht, _ptr(leaf), leaf.size, _ptr(out)) != 0:
+        raise ValueError(f"unsupported hash type {ht}")
+    return out
+
+
+def hash_two(ht: int, left: np.ndarray, right: np.ndarray) -> np.ndarray:
+    out = np.zeros(4, dtype=np.uint64)
+    l = np.ascontiguousarray(left, dtype=np.uint64)
+    r = np.ascontiguousarray(right, dtype=np.uint64)
+    if lib().orc_hash_two(ht, _ptr(l), _ptr(r), _ptr(out)) != 0:
+        raise ValueError(f"unsupported hash type {ht}")
+    return out
+
+
+def permute(ht: int, state: np.ndarray) -> np.ndarray:
+    st = np.ascontiguousarray(state, dtype=np.uint64).copy()
+    assert st.size == 12
+    (lib().orc_poseidon_permute if ht == HASH_POSEIDON else lib().orc_poseidon2_permute)(_ptr(st))
+    return st
+
+
+def merkle_sizes(n_leaves: int, cap_height: int):
+    n_caps = 1 << cap_height
+    return 2 * (n_leaves - n_caps), n_caps
+
+
+def merkle_fill(leaves: np.ndarray, leaf_size: int, cap_height: int, ht: int,
+                digests: np.ndarray | None = None, cap: np.ndarray | None = None):
+    """Digests + cap in zeknox's linear layout (merkle/merkle.cu:166-244)."""
+    leaves = np.ascontiguousarray(leaves, dtype=np.uint64).reshape(-1)
+    n_leaves = leaves.size // leaf_size
+    n_digests, n_caps = merkle_sizes(n_leaves, cap_height)
+    if digests is None:
+        digests = np.zeros(max(n_digests, 1) * 4, dtype=np.uint64)
+    if cap is None:
+        cap = np.zeros(n_caps * 4, dtype=np.uint64)
+    rc = lib().orc_merkle_fill(_ptr(digests), _ptr(cap), _ptr(leaves), n_digests, n_caps, n_leaves,
+                               leaf_size, cap_height, ht)
+    if rc != 0:
+        raise ValueError(f"unsupported hash type {ht}")
+    return digests, cap
+
+
+def ref_merkle_fill(leaves: np.ndarray, leaf_size: int, cap_height: int, ht: int):
+    """zeknox's own fill_digests_buf_linear_cpu (merkle/merkle.cpp:126-161)."""
+    R = ref()
+    if R is None:
+        raise RuntimeError("zeknox CPU build not available (oracle/build_ref.sh)")
+    leaves = np.ascontiguousarray(leaves, dtype=np.uint64).reshape(-1)
+    n_leaves = leaves.size // leaf_size
+    n_digests, n_caps = merkle_sizes(n_leaves, cap_height)
+    digests = np.zeros(max(n_digests, 1) * 4, dtype=np.uint64)
+    cap = np.zeros(n_caps * 4, dtype=np.uint64)
+    R.fill_digests_buf_linear_cpu(digests.ctypes.data, cap.ctypes.data, leaves.ctypes.data, n_digests,
+                                  n_caps, n_leaves, leaf_size, cap_height, ht)
+    return digests, cap
+
+
+# ---------------------------------------------------------------- NTT
+def ntt_raw(a: np.ndarray, lg: int, inverse: bool = False) -> np.ndarray:
+    out = np.ascontiguousarray(a, dtype=np.uint64).copy()
+    lib().orc_ntt_raw(_ptr(out), lg, int(inverse))
+    return out
+
+
+def batch_ntt(inout: np.ndarray, lg: int, inverse: bool, batches: int, with_coset: bool = False,
+              coset_gen: int = 7) -> np.ndarray:
+    out = np.ascontiguousarray(inout, dtype=np.uint64).copy()
+    assert out.size == batches << lg
+    lib().orc_batch_ntt(_ptr(out), lg, int(inverse), batches, int(with_coset), coset_gen)
+    return out
+
+
+def batch_lde(inp: np.ndarray, lg_n: int, rate_bits: int, batches: int, inverse: bool = False,
+              with_coset: bool = True, coset_gen: int = 7) -> np.ndarray:
+    inp = np.ascontiguousarray(inp, dtype=np.uint64)
+    assert inp.size == batches << lg_n
+    out = np.empty(batches << (lg_n + rate_bits), dtype=np.uint64)
+    lib().orc_batch_lde(_ptr(out), _ptr(inp), lg_n, rate_bits, int(inverse), batches, int(with_coset), coset_gen)
+    return out
+
+
+def transpose_rev(inp: np.ndarray, lg_n: int, batches: int) -> np.ndarray:
+    inp = np.ascontiguousarray(inp, dtype=np.uint64)
+    assert inp.size == batches << lg_n
+    out = np.empty_like(inp)
+    lib().orc_transpose_rev(_ptr(out), _ptr(inp), lg_n, batches)
+    return out
+
+
+def set_threads(n: int) -> None:
+    os.environ["OMP_NUM_THREADS"] = str(n)

@@ -1,0 +1,225 @@
+"""GPU parity: NTT / coset LDE / bit-reversing transpose through the C ABI,
+bit-exact against the oracle (and against zeknox's own sm_100a build when
+oracle/_ref/libzkref_gpu.so was built)."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def zk():
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import zeknox_b200 as zk
+
+    return zk
+
+
+def _dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _host(t):
+    import torch
+
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def _cfg(zk, batches, rate=0, in_dev=False, out_dev=False, coset=False, salt=0):
+    c = zk.NTTConfig.default()
+    c.batches = batches
+    c.extension_rate_bits = rate
+    c.are_inputs_on_device = in_dev
+    c.are_outputs_on_device = out_dev
+    c.with_coset = coset
+    c.salt_size = salt
+    return c
+
+
+LDE_CASES = [(1, 1, 1), (2, 1, 3), (4, 2, 5), (6, 3, 2), (9, 1, 4), (10, 3, 3), (11, 2, 2), (12, 1, 2),
+             (13, 3, 2), (15, 3, 4), (16, 3, 1), (20, 1, 1), (21, 3, 1), (22, 3, 1)]
+
+
+@pytest.mark.parametrize("lg_n,rate,batches", LDE_CASES)
+def test_lde_host_buffers(zk, oracle, lg_n, rate, batches):
+    x = oracle.field_elems(1000 + lg_n * 10 + rate, batches << lg_n)
+    out = np.zeros(batches << (lg_n + rate), dtype=np.uint64)
+    zk.lde_batch(0, out.ctypes.data, x.ctypes.data, lg_n, _cfg(zk, batches, rate, coset=True))
+    assert np.array_equal(out, oracle.batch_lde(x, lg_n, rate, batches))
+
+
+@pytest.mark.parametrize("lg_n,rate,batches,inverse,coset", [
+    (5, 2, 3, False, False), (5, 2, 3, True, True), (5, 2, 3, True, False), (12, 2, 2, True, True),
+    (14, 3, 3, False, False), (14, 3, 3, True, True)])
+def test_lde_device_buffers_and_directions(zk, oracle, lg_n, rate, batches, inverse, coset):
+    x = oracle.field_elems(2000 + lg_n, batches << lg_n)
+    d_in = _dev(x)
+    d_out = _dev(np.zeros(batches << (lg_n + rate), dtype=np.uint64))
+    zk.lde_batch(0, d_out.data_ptr(), d_in.data_ptr(), lg_n, _cfg(zk, batches, rate, True, True, coset),
+                 zk.INVERSE if inverse else zk.FORWARD)
+    exp = oracle.batch_lde(x, lg_n, rate, batches, inverse=inverse, with_coset=coset)
+    assert np.array_equal(_host(d_out), exp)
+    assert np.array_equal(_host(d_in), x)  # input untouched
+
+
+def test_lde_mixed_host_device(zk, oracle):
+    lg_n, rate, b = 11, 2, 3
+    x = oracle.field_elems(3, b << lg_n)
+    exp = oracle.batch_lde(x, lg_n, rate, b)
+    d_out = _dev(np.zeros(b << (lg_n + rate), dtype=np.uint64))
+    zk.lde_batch(0, d_out.data_ptr(), x.ctypes.data, lg_n, _cfg(zk, b, rate, False, True, True))
+    assert np.array_equal(_host(d_out), exp)
+    out = np.zeros_like(exp)
+    d_in = _dev(x)
+    zk.lde_batch(0, out.ctypes.data, d_in.data_ptr(), lg_n, _cfg(zk, b, rate, True, False, True))
+    assert np.array_equal(out, exp)
+
+
+def test_lde_salt_rows(zk, oracle):
+    # ntt.cu:541-545: salt_size extra rows of random field elements after the LDE rows
+    lg_n, rate, b, salt = 8, 2, 2, 3
+    x = oracle.field_elems(4, b << lg_n)
+    N = 1 << (lg_n + rate)
+    out = np.zeros((b + salt) * N, dtype=np.uint64)
+    zk.lde_batch(0, out.ctypes.data, x.ctypes.data, lg_n, _cfg(zk, b, rate, coset=True, salt=salt))
+    assert np.array_equal(out[: b * N], oracle.batch_lde(x, lg_n, rate, b))
+    s = out[b * N:]
+    assert (s < np.uint64(oracle.P)).all() and len(np.unique(s)) > 0.99 * s.size
+
+
+def test_lde_invalid_args(zk):
+    with pytest.raises(zk.ZeknoxError) as e:
+        zk.lde_batch(0, 0, 0, 0, _cfg(zk, 1, 1))
+    assert e.value.code == 1
+    with pytest.raises(zk.ZeknoxError):
+        zk.lde_batch(0, 0, 0, 4, _cfg(zk, 1, 0))
+
+
+NTT_CASES = [1, 2, 5, 11, 12, 13, 17, 18, 23]
+
+
+@pytest.mark.parametrize("lg", NTT_CASES)
+@pytest.mark.parametrize("coset", [False, True])
+def test_batch_ntt_forward_inverse(zk, oracle, lg, coset):
+    batches = 3 if lg <= 18 else 1
+    x = oracle.field_elems(500 + lg, batches << lg)
+    a = x.copy()
+    zk.ntt_batch(0, a.ctypes.data, lg, _cfg(zk, batches, coset=coset))
+    assert np.array_equal(a, oracle.batch_ntt(x, lg, False, batches, coset))
+    d = _dev(x)
+    zk.intt_batch(0, d.data_ptr(), lg, _cfg(zk, batches, in_dev=True, out_dev=True, coset=coset))
+    assert np.array_equal(_host(d), oracle.batch_ntt(x, lg, True, batches, coset))
+
+
+def test_ntt_three_pass_vs_oracle(zk, oracle):
+    lg = 25  # three shared-memory passes
+    x = oracle.field_elems(25, 1 << lg)
+    d = _dev(x)
+    zk.ntt_batch(0, d.data_ptr(), lg, _cfg(zk, 1, in_dev=True, out_dev=True, coset=True))
+    assert np.array_equal(_host(d), oracle.batch_ntt(x, lg, False, 1, True))
+
+
+def test_ntt_roundtrip_large(zk, oracle):
+    # size-independent property at 2^26: iNTT(NTT(x)) == x
+    lg, b = 26, 1
+    x = oracle.field_elems(77, b << lg)
+    d = _dev(x)
+    zk.ntt_batch(0, d.data_ptr(), lg, _cfg(zk, b, in_dev=True, out_dev=True))
+    zk.intt_batch(0, d.data_ptr(), lg, _cfg(zk, b, in_dev=True, out_dev=True))
+    assert np.array_equal(_host(d), x)
+
+
+def test_init_coset_other_generator(zk, oracle):
+    lg = 10
+    zk.init_coset(0, lg, 11)
+    try:
+        x = oracle.field_elems(8, 2 << lg)
+        a = x.copy()
+        zk.ntt_batch(0, a.ctypes.data, lg, _cfg(zk, 2, coset=True))
+        assert np.array_equal(a, oracle.batch_ntt(x, lg, False, 2, True, 11))
+    finally:
+        zk.init_coset(0, 20, 7)
+
+
+@pytest.mark.parametrize("lg,batches", [(0, 1), (1, 3), (5, 7), (10, 135), (13, 16), (18, 135), (6, 1000)])
+def test_transpose_rev(zk, oracle, lg, batches):
+    x = oracle.field_elems(9 + lg, batches << lg)
+    out = np.zeros_like(x)
+    c = zk.TransposeConfig.default()
+    c.batches = batches
+    zk.transpose_rev_batch(0, out.ctypes.data, x.ctypes.data, lg, c)
+    assert np.array_equal(out, oracle.transpose_rev(x, lg, batches))
+    d_in, d_out = _dev(x), _dev(np.zeros_like(x))
+    c.are_inputs_on_device = c.are_outputs_on_device = True
+    zk.transpose_rev_batch(0, d_out.data_ptr(), d_in.data_ptr(), lg, c)
+    assert np.array_equal(_host(d_out), out)
+
+
+def test_lde_multi_gpu_entry(zk, oracle):
+    lg_n, rate, b = 10, 2, 5
+    x = oracle.field_elems(12, b << lg_n)
+    d_out = _dev(np.zeros(b << (lg_n + rate), dtype=np.uint64))
+    zk.lde_batch_multi_gpu(d_out.data_ptr(), x.ctypes.data, 1, _cfg(zk, b, rate, coset=True), lg_n, x.size,
+                           b << (lg_n + rate))
+    assert np.array_equal(_host(d_out), oracle.batch_lde(x, lg_n, rate, b))
+
+
+# ---------------------------------------------- zeknox's own sm_100a build
+def _ref_gpu():
+    from oracle.oracle import HERE
+
+    so = HERE / "_ref" / "libzkref_gpu.so"
+    if not so.exists():
+        pytest.skip("zeknox sm_100a build not present (oracle/build_ref.sh)")
+    from zeknox_b200.capi import NTTConfig, RustError, TransposeConfig
+
+    L = ctypes.CDLL(str(so))
+    vp, sz, u32, u64 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64
+    L.init_twiddle_factors.argtypes = [sz, sz]
+    L.init_twiddle_factors.restype = RustError
+    L.init_coset.argtypes = [sz, sz, u64]
+    L.init_coset.restype = RustError
+    L.compute_batched_lde.argtypes = [sz, vp, vp, u32, ctypes.c_int, NTTConfig]
+    L.compute_batched_lde.restype = RustError
+    L.compute_batched_ntt.argtypes = [sz, vp, u32, ctypes.c_int, NTTConfig]
+    L.compute_batched_ntt.restype = RustError
+    L.compute_transpose_rev.argtypes = [sz, vp, vp, u32, TransposeConfig]
+    L.compute_transpose_rev.restype = RustError
+    L.fill_digests_buf_linear_gpu_with_gpu_ptr.argtypes = [vp, vp, vp, u64, u64, u64, u64, u64, u64, u64]
+    L.fill_digests_buf_linear_gpu_with_gpu_ptr.restype = None
+    return L
+
+
+@pytest.mark.parametrize("lg_n,rate,batches", [(4, 1, 2), (12, 3, 5), (15, 3, 8)])
+def test_lde_vs_zeknox_sm100_build(zk, oracle, lg_n, rate, batches):
+    R = _ref_gpu()
+    lg = lg_n + rate
+    assert R.init_twiddle_factors(0, lg).code == 0
+    assert R.init_coset(0, lg, 7).code == 0
+    x = oracle.field_elems(42 + lg, batches << lg_n)
+    ref_out = np.zeros(batches << lg, dtype=np.uint64)
+    c = _cfg(zk, batches, rate, coset=True)
+    assert R.compute_batched_lde(0, ref_out.ctypes.data, x.ctypes.data, lg_n, 0, c).code == 0
+    out = np.zeros_like(ref_out)
+    zk.lde_batch(0, out.ctypes.data, x.ctypes.data, lg_n, c)
+    assert np.array_equal(out, ref_out)
+
+
+def test_transpose_vs_zeknox_sm100_build(zk, oracle):
+    R = _ref_gpu()
+    lg, b = 14, 135
+    x = oracle.field_elems(5, b << lg)
+    c = zk.TransposeConfig.default()
+    c.batches = b
+    ref_out, out = np.zeros_like(x), np.zeros_like(x)
+    assert R.compute_transpose_rev(0, ref_out.ctypes.data, x.ctypes.data, lg, c).code == 0
+    zk.transpose_rev_batch(0, out.ctypes.data, x.ctypes.data, lg, c)
+    assert np.array_equal(out, ref_out)

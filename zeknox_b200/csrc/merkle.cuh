@@ -1,0 +1,21 @@
+// Host interface of the Merkle builder (merkle.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace zk {
+
+// Sizes as in zeknox's fill_digests_buf_linear_* (native/merkle/merkle.h:30-62):
+// counts of 4-element digests and of leaves; all pointers on the device.
+struct MerkleJob {
+    uint64_t *digests = nullptr;
+    uint64_t *cap = nullptr;
+    const uint64_t *leaves = nullptr;
+    uint64_t n_digests = 0, n_caps = 0, n_leaves = 0, leaf_size = 0, cap_height = 0, hash_type = 0;
+};
+
+bool merkle_hash_supported(uint64_t hash_type);
+void merkle_validate(const MerkleJob &job);  // throws zk::Error
+void merkle_run(const MerkleJob &job, cudaStream_t s);
+
+}  // namespace zk

@@ -1,0 +1,411 @@
+// Batched NTT / coset LDE / bit-reversing transpose for sm_100a.
+//
+// zeknox (native/ntt/ntt.cu:106-158, kernels.cu:14-392) runs one global
+// radix-2 stage per launch plus bit-reversal, zero-extension, coset and
+// normalisation passes.  Here a size-2^lg transform is split into P <= 3
+// passes (lg = l_1 + ... + l_P, each l_p <= 12); every pass moves a group of
+// lines (strided columns, or contiguous rows in the last pass) into shared
+// memory, runs a 2^l_p-point transform there, applies the inter-pass twiddle
+// and writes back, so the whole transform costs P reads and P writes of the
+// data.  Zero-extension, the coset multiply and the 1/N scaling are folded
+// into the first / last pass, and the last pass writes natural order directly
+// (no bit-reversal pass).
+//
+// Decomposition (Cooley-Tukey over mixed radix): with N = N_1 * S_1,
+//   X[k_1 + N_1 k'] = sum_r w_{S_1}^{r k'} [ w_N^{r k_1} sum_i x[i S_1 + r] w_{N_1}^{i k_1} ]
+// pass 1 computes the bracket for every column r (stride S_1) in place, the
+// remaining passes transform each contiguous block of S_1 elements the same
+// way, and the last pass stores X at its natural index.
+#include <stdint.h>
+
+#include <algorithm>
+#include <atomic>
+
+#include "gl64.cuh"
+#include "ntt.cuh"
+#include "runtime.cuh"
+
+namespace zk {
+
+namespace {
+
+constexpr int kNttThreads = 256;
+constexpr int kLinesElems = 1 << 13;  // elements per group held in shared memory
+
+struct PassArgs {
+    const uint64_t *src;
+    uint64_t *dst;
+    uint64_t src_poly_stride;  // elements between consecutive polynomials
+    uint64_t dst_poly_stride;
+    uint32_t batches;
+    uint32_t lg_n;      // log2 of the transform size N
+    uint32_t l;         // log2 line length L of this pass
+    uint32_t lg_s;      // log2 stride S of line elements (column pass); 0 in the last pass
+    uint32_t lg_pre;    // log2 of the number of prefixes Q = N / (L * S)
+    uint32_t lg_t;      // log2 lines per group T
+    uint32_t l_first;   // log2 N_1 (digit split of the prefix, 3-pass last pass)
+    uint32_t kind;      // 0 column pass, 1 last pass (rows), 2 single pass
+    // first pass: zero-extension and coset pre-multiply
+    uint64_t n_valid;   // source elements per polynomial that are read (others are 0)
+    const uint64_t *pre_lo, *pre_hi;  // coset powers (null: none)
+    uint32_t pre_h;
+    // last pass: output scaling by coset^k * scale
+    const uint64_t *post_lo, *post_hi;  // coset powers (null: none)
+    uint32_t post_h;
+    uint64_t scale;     // 1 = none
+    // twiddles
+    const uint64_t *tw_lo, *tw_hi;  // omega_N powers (two-level)
+    uint32_t tw_h;
+    const uint64_t *line_roots;     // omega_4096^j, j < 2048
+};
+
+__device__ __forceinline__ uint64_t pow2l(const uint64_t *lo, const uint64_t *hi, uint32_t h, uint64_t e) {
+    return gl_mul(__ldg(lo + (e & ((1ull << h) - 1))), __ldg(hi + (e >> h)));
+}
+
+__device__ __forceinline__ uint32_t brev_bits(uint32_t x, uint32_t bits) {
+    return bits ? (__brev(x) >> (32 - bits)) : 0u;
+}
+
+// In-place radix-2 DIF over T interleaved lines of length L in shared memory
+// (element e of line t at e * tp + t).  Natural order in, bit-reversed out.
+__device__ __forceinline__ void smem_dif(uint64_t *sm, const uint64_t *tw, uint32_t l, uint32_t T, uint32_t tp) {
+    const uint32_t L = 1u << l;
+    const uint32_t nb = (T * L) >> 1;
+    for (int s = (int)l - 1; s >= 0; s--) {
+        __syncthreads();
+        const uint32_t h = 1u << s;
+        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {
+            const uint32_t t = b % T, j = b / T;
+            const uint32_t o = j & (h - 1);
+            const uint32_t e0 = ((j >> s) << (s + 1)) + o;
+            const uint32_t i0 = e0 * tp + t, i1 = (e0 + h) * tp + t;
+            const uint64_t u = sm[i0], v = sm[i1];
+            sm[i0] = gl_add(u, v);
+            const uint64_t d = gl_sub(u, v);
+            sm[i1] = o ? gl_mul(d, tw[o << (l - 1 - s)]) : d;
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
+    extern __shared__ uint64_t smem[];
+    const uint32_t l = a.l, L = 1u << l;
+    const uint32_t T = 1u << a.lg_t;
+    const uint32_t tp = T > 1 ? T + 1 : 1;
+    uint64_t *tw = smem;              // L/2 line roots
+    uint64_t *sm = smem + (L >> 1 > 0 ? L >> 1 : 1);
+    // line roots omega_L^j = omega_4096^(j * 4096 / L)
+    for (uint32_t j = threadIdx.x; j < (L >> 1); j += blockDim.x) tw[j] = __ldg(a.line_roots + (j << (kLineLgMax - l)));
+
+    const uint64_t N = 1ull << a.lg_n;
+    uint64_t g = blockIdx.x;
+
+    if (a.kind == 0) {
+        // ---- column pass: lines r0 + t (t < T) of prefix q, elements at stride S
+        const uint32_t lg_s = a.lg_s;
+        const uint64_t S = 1ull << lg_s;
+        const uint64_t groups_per_prefix = S >> a.lg_t;
+        const uint64_t groups_per_poly = groups_per_prefix << a.lg_pre;
+        const uint64_t poly = g / groups_per_poly;
+        const uint64_t rem = g % groups_per_poly;
+        const uint64_t q = rem / groups_per_prefix;
+        const uint64_t r0 = (rem % groups_per_prefix) << a.lg_t;
+        const uint64_t base = q << (l + lg_s);  // prefix block start within the polynomial
+        const uint64_t *src = a.src + poly * a.src_poly_stride;
+        uint64_t *dst = a.dst + poly * a.dst_poly_stride;
+        for (uint32_t idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
+            const uint32_t t = idx & (T - 1), e = idx >> a.lg_t;
+            const uint64_t i = base + ((uint64_t)e << lg_s) + r0 + t;  // index within the polynomial
+            uint64_t v = 0;
+            if (i < a.n_valid) {
+                v = gl_canon(src[i]);
+                if (a.pre_lo) v = gl_mul(v, pow2l(a.pre_lo, a.pre_hi, a.pre_h, i));
+            }
+            sm[e * tp + t] = v;
+        }
+        __syncthreads();
+        smem_dif(sm, tw, l, T, tp);
+        for (uint32_t idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
+            const uint32_t t = idx & (T - 1), k = idx >> a.lg_t;
+            uint64_t v = sm[brev_bits(k, l) * tp + t];
+            const uint64_t e = ((r0 + t) * (uint64_t)k) << a.lg_pre;  // w_{L S}^{r k} = w_N^{r k Q}
+            if (e) v = gl_mul(v, pow2l(a.tw_lo, a.tw_hi, a.tw_h, e));
+            dst[base + ((uint64_t)k << lg_s) + r0 + t] = v;
+        }
+        return;
+    }
+
+    // ---- row passes: T lines, each a contiguous run of L elements
+    const uint64_t Q = 1ull << a.lg_pre;  // prefixes per polynomial (1 for a single pass)
+    uint64_t poly0, c0;
+    uint32_t nlines = T;
+    if (a.kind == 1) {
+        const uint64_t groups_per_poly = Q >> a.lg_t;
+        poly0 = g / groups_per_poly;
+        c0 = (g % groups_per_poly) << a.lg_t;  // first digit-reversed prefix of the group
+    } else {
+        poly0 = g << a.lg_t;
+        c0 = 0;
+        if (poly0 + T > a.batches) nlines = (uint32_t)(a.batches - poly0);
+    }
+    auto line_src = [&](uint32_t t) -> uint64_t {  // element offset of line t's start in src
+        if (a.kind == 2) return (poly0 + t) * a.src_poly_stride;
+        const uint64_t krev = c0 + t;  // k_1 + N_1 k_2 (3 passes) or k_1 (2 passes)
+        const uint64_t mask1 = (1ull << a.l_first) - 1;
+        const uint64_t kpos = ((krev & mask1) << (a.lg_pre - a.l_first)) | (krev >> a.l_first);
+        return poly0 * a.src_poly_stride + (kpos << l);
+    };
+    for (uint32_t idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
+        const uint32_t e = idx & (L - 1), t = idx >> l;
+        uint64_t v = 0;
+        if (t < nlines) {
+            if (a.kind == 2) {
+                if (e < a.n_valid) {
+                    v = gl_canon(a.src[line_src(t) + e]);
+                    if (a.pre_lo) v = gl_mul(v, pow2l(a.pre_lo, a.pre_hi, a.pre_h, e));
+                }
+            } else {
+                v = a.src[line_src(t) + e];
+            }
+        }
+        sm[e * tp + t] = v;
+    }
+    __syncthreads();
+    smem_dif(sm, tw, l, T, tp);
+    if (a.kind == 1) {
+        // natural index of line t's element k: krev + Q * k
+        uint64_t *dst = a.dst + poly0 * a.dst_poly_stride;
+        for (uint32_t idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
+            const uint32_t t = idx & (T - 1), k = idx >> a.lg_t;
+            uint64_t v = sm[brev_bits(k, l) * tp + t];
+            const uint64_t o = c0 + t + ((uint64_t)k << a.lg_pre);
+            if (a.post_lo) v = gl_mul(v, pow2l(a.post_lo, a.post_hi, a.post_h, o));
+            if (a.scale != 1) v = gl_mul(v, a.scale);
+            dst[o] = v;
+        }
+    } else {
+        for (uint32_t idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
+            const uint32_t k = idx & (L - 1), t = idx >> l;
+            if (t >= nlines) continue;
+            uint64_t v = sm[brev_bits(k, l) * tp + t];
+            if (a.post_lo) v = gl_mul(v, pow2l(a.post_lo, a.post_hi, a.post_h, k));
+            if (a.scale != 1) v = gl_mul(v, a.scale);
+            a.dst[(poly0 + t) * a.dst_poly_stride + k] = v;
+        }
+    }
+    (void)N;
+}
+
+// out[rev(k) * B + b] = in[b * N + k]: 16 rows x 64 columns per block, through
+// shared memory so both sides are coalesced (zeknox kernels.cu:94-135).
+constexpr int kTrRows = 16, kTrCols = 64;
+__global__ void __launch_bounds__(256) transpose_rev_kernel(uint64_t *__restrict__ out, const uint64_t *__restrict__ in,
+                                                            uint32_t lg_n, uint32_t batches) {
+    __shared__ uint64_t tile[kTrCols * (kTrRows + 1)];
+    const uint64_t N = 1ull << lg_n;
+    const uint64_t k0 = (uint64_t)blockIdx.x * kTrCols;
+    const uint32_t b0 = blockIdx.y * kTrRows;
+    for (uint32_t idx = threadIdx.x; idx < kTrRows * kTrCols; idx += blockDim.x) {
+        const uint32_t bl = idx / kTrCols, kl = idx % kTrCols;
+        if (b0 + bl < batches && k0 + kl < N) tile[kl * (kTrRows + 1) + bl] = in[(uint64_t)(b0 + bl) * N + k0 + kl];
+    }
+    __syncthreads();
+    for (uint32_t idx = threadIdx.x; idx < kTrRows * kTrCols; idx += blockDim.x) {
+        const uint32_t kl = idx / kTrRows, bl = idx % kTrRows;
+        const uint64_t k = k0 + kl;
+        if (b0 + bl < batches && k < N) {
+            const uint64_t r = lg_n ? (__brevll(k) >> (64 - lg_n)) : 0;
+            out[r * batches + b0 + bl] = tile[kl * (kTrRows + 1) + bl];
+        }
+    }
+}
+
+// Salt rows: uniform field elements from a counter-based SplitMix64 stream.
+__global__ void salt_kernel(uint64_t *out, uint64_t count, uint64_t seed) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t ctr = i, z;
+        do {
+            z = seed + (ctr + 1) * 0x9E3779B97F4A7C15ull;
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+            z ^= z >> 31;
+            ctr += count;
+        } while (z >= ZK_P);
+        out[i] = z;
+    }
+}
+
+struct Plan {
+    int passes;
+    uint32_t l[3];
+};
+
+Plan make_plan(uint32_t lg) {
+    Plan p{};
+    if (lg <= 12) {
+        p.passes = 1;
+        p.l[0] = lg;
+    } else if (lg <= 24) {
+        p.passes = 2;
+        p.l[0] = (lg + 1) / 2;
+        p.l[1] = lg - p.l[0];
+    } else {
+        p.passes = 3;
+        p.l[0] = (lg + 2) / 3;
+        p.l[1] = (lg - p.l[0] + 1) / 2;
+        p.l[2] = lg - p.l[0] - p.l[1];
+    }
+    return p;
+}
+
+uint32_t ilog2_floor(uint64_t x) { return 63 - __builtin_clzll(x); }
+
+size_t pass_smem(uint32_t l, uint32_t lg_t) {
+    const uint64_t T = 1ull << lg_t, tp = T > 1 ? T + 1 : 1;
+    const uint64_t L = 1ull << l;
+    return (size_t)(std::max<uint64_t>(L >> 1, 1) + L * tp) * sizeof(uint64_t);
+}
+
+void launch_pass(const PassArgs &a, uint64_t groups, cudaStream_t s) {
+    const size_t smem = pass_smem(a.l, a.lg_t);
+    static std::atomic<uint64_t> attr_set{0};  // one bit per device
+    const int dev = current_device();
+    if (dev < 64 && !(attr_set.load() & (1ull << dev))) {
+        ZK_CUDA(cudaFuncSetAttribute(ntt_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        attr_set.fetch_or(1ull << dev);
+    }
+    require(groups < (1ull << 31), "transform too large for one launch");
+    ntt_pass_kernel<<<(unsigned)groups, kNttThreads, smem, s>>>(a);
+    ZK_CHECK_LAUNCH();
+}
+
+}  // namespace
+
+// One batched transform of `batches` polynomials of 2^lg elements.
+void ntt_run(const NttJob &j, cudaStream_t s) {
+    const uint32_t lg = j.lg;
+    require(lg >= 1 && lg <= 32, "transform size out of range");
+    if (j.batches == 0) return;
+    DeviceCtx &ctx = device_ctx(current_device());
+    const PowTable &rt = root_table(ctx, lg, j.inverse);
+    const uint64_t *lr = line_roots(ctx, j.inverse);
+    const Plan plan = make_plan(lg);
+    const uint64_t N = 1ull << lg;
+
+    PassArgs base{};
+    base.lg_n = lg;
+    base.tw_lo = rt.lo();
+    base.tw_hi = rt.hi();
+    base.tw_h = rt.h;
+    base.line_roots = lr;
+    base.scale = j.scale;
+    base.batches = j.batches;
+    if (j.pre_coset) {
+        base.pre_lo = j.pre_coset->lo();
+        base.pre_hi = j.pre_coset->hi();
+        base.pre_h = j.pre_coset->h;
+    }
+    if (j.post_coset) {
+        base.post_lo = j.post_coset->lo();
+        base.post_hi = j.post_coset->hi();
+        base.post_h = j.post_coset->h;
+    }
+
+    if (plan.passes == 1) {
+        PassArgs a = base;
+        a.kind = 2;
+        a.l = lg;
+        a.lg_pre = 0;
+        a.lg_t = std::min<uint32_t>(ilog2_floor(kLinesElems) - lg, 6);
+        a.src = j.src;
+        a.dst = j.dst;
+        a.src_poly_stride = j.src_stride;
+        a.dst_poly_stride = j.dst_stride;
+        a.n_valid = j.n_valid;
+        const uint64_t groups = (j.batches + (1ull << a.lg_t) - 1) >> a.lg_t;
+        launch_pass(a, groups, s);
+        return;
+    }
+
+    // Multi-pass: process polynomials in chunks whose intermediate (chunk * N
+    // elements) stays within `scratch_elems`, so it is L2-resident when small.
+    const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(j.batches, j.scratch_elems / N));
+    uint64_t *scr = j.scratch;
+    for (uint64_t b0 = 0; b0 < j.batches; b0 += chunk) {
+        const uint64_t nb = std::min<uint64_t>(chunk, j.batches - b0);
+        uint32_t lg_s = lg;
+        for (int p = 0; p < plan.passes; p++) {
+            PassArgs a = base;
+            a.l = plan.l[p];
+            a.l_first = plan.l[0];
+            a.batches = (uint32_t)nb;
+            if (p < plan.passes - 1) {
+                lg_s -= a.l;
+                a.kind = 0;
+                a.lg_s = lg_s;
+                a.lg_pre = lg - a.l - lg_s;
+                a.lg_t = std::min<uint32_t>(ilog2_floor(kLinesElems) - a.l, lg_s);
+                a.lg_t = std::min<uint32_t>(a.lg_t, 5);
+                if (p == 0) {
+                    a.src = j.src + b0 * j.src_stride;
+                    a.src_poly_stride = j.src_stride;
+                    a.n_valid = j.n_valid;
+                } else {
+                    a.src = scr;
+                    a.src_poly_stride = N;
+                    a.n_valid = N;
+                    a.pre_lo = nullptr;
+                }
+                a.dst = scr;
+                a.dst_poly_stride = N;
+                a.post_lo = nullptr;
+                a.scale = 1;
+                const uint64_t groups = nb << (lg - a.l - a.lg_t);
+                launch_pass(a, groups, s);
+            } else {
+                a.kind = 1;
+                a.lg_s = 0;
+                a.lg_pre = lg - a.l;
+                a.lg_t = std::min<uint32_t>(ilog2_floor(kLinesElems) - a.l, plan.l[0]);
+                a.lg_t = std::min<uint32_t>(a.lg_t, 5);
+                a.src = scr;
+                a.src_poly_stride = N;
+                a.dst = j.dst + b0 * j.dst_stride;
+                a.dst_poly_stride = j.dst_stride;
+                a.pre_lo = nullptr;
+                a.n_valid = N;
+                const uint64_t groups = nb << (a.lg_pre - a.lg_t);
+                launch_pass(a, groups, s);
+            }
+        }
+    }
+}
+
+uint64_t ntt_scratch_elems(uint32_t lg, uint64_t batches) {
+    if (make_plan(lg).passes == 1) return 0;
+    const uint64_t N = 1ull << lg;
+    // At most 32 MiB of intermediate (fits in L2 next to the streamed data),
+    // but always at least one polynomial.
+    const uint64_t cap = (32ull << 20) / sizeof(uint64_t);
+    return std::max<uint64_t>(N, std::min<uint64_t>(batches * N, cap / N * N));
+}
+
+void transpose_rev_run(uint64_t *out, const uint64_t *in, uint32_t lg_n, uint32_t batches, cudaStream_t s) {
+    if (batches == 0) return;
+    const uint64_t N = 1ull << lg_n;
+    const uint64_t gx = (N + kTrCols - 1) / kTrCols;
+    require(gx < (1ull << 31) && (batches + kTrRows - 1) / kTrRows < 65536, "transpose too large");
+    dim3 grid((unsigned)gx, (batches + kTrRows - 1) / kTrRows);
+    transpose_rev_kernel<<<grid, 256, 0, s>>>(out, in, lg_n, batches);
+    ZK_CHECK_LAUNCH();
+}
+
+void salt_run(uint64_t *out, uint64_t count, uint64_t seed, cudaStream_t s) {
+    if (!count) return;
+    salt_kernel<<<1184, 256, 0, s>>>(out, count, seed);
+    ZK_CHECK_LAUNCH();
+}
+
+}  // namespace zk
