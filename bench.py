@@ -31,21 +31,34 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "Goldilocks LDE+Merkle commit elems/s, batched vs plain, bit-exact; p99 latency"
-B, LG_N, RATE, CAP_H = 135, 15, 3, 4
-LG = LG_N + RATE
-N = 1 << LG
-n = 1 << LG_N
-HASH = 0  # Poseidon
-N_ROT = 4  # rotating input buffers: 4 x 35 MB > L2 (126 MB)
 P = 0xFFFFFFFF00000001
-WORKLOAD = f"commit: LDE {B}x2^{LG_N} rate {RATE} coset 7 -> transpose_rev -> Poseidon Merkle cap_height {CAP_H}"
-# Algorithmic work per step.
-LEAF_PERMS = N * ((B + 7) // 8)
-NODE_PERMS = (1 << CAP_H) * ((N >> CAP_H) - 2) + (1 << CAP_H)  # internal nodes + cap entries
-PERMS = LEAF_PERMS + NODE_PERMS
-POSEIDON_OPS = 15378  # INT32 multiply-class ops per permutation (fast-partial-round accounting)
-LDE_BYTES = 8 * B * (n + N)
-TRANSPOSE_BYTES = 16 * B * N
+HASH_NAMES = {"poseidon": 0, "keccak": 1, "poseidon2": 3}
+# INT32 multiply-class ops per permutation (a 64x64 mulmod counts 10, a
+# small-constant MAC 4): Poseidon 1077 mulmod + 1152 MAC, Poseidon2 736 mulmod,
+# Keccak-f 3720 64-bit logic ops counted as 2 each.
+OPS_PER_PERM = {0: 15378, 3: 7360, 1: 7440}
+
+
+def set_workload(polys=135, lg_n=15, rate=3, cap_h=4, hash_name="poseidon", rot=4):
+    """Workload of one step; the defaults are the plain single-job commit
+    (135 x 2^15 coefficients, rate 3, Poseidon, cap height 4)."""
+    global B, LG_N, RATE, CAP_H, LG, N, n, HASH, HASH_NAME, N_ROT, WORKLOAD, LEAF_PERMS, NODE_PERMS, PERMS
+    global LDE_BYTES, TRANSPOSE_BYTES
+    B, LG_N, RATE, CAP_H, HASH_NAME, N_ROT = polys, lg_n, rate, cap_h, hash_name, rot
+    HASH = HASH_NAMES[hash_name]
+    LG = LG_N + RATE
+    N, n = 1 << LG, 1 << LG_N
+    WORKLOAD = (f"commit: LDE {B}x2^{LG_N} rate {RATE} coset 7 -> transpose_rev -> {hash_name} Merkle "
+                f"cap_height {CAP_H}")
+    rate_words = 17 if HASH == 1 else 8  # elements absorbed per permutation
+    LEAF_PERMS = N * ((B + rate_words - 1) // rate_words)
+    NODE_PERMS = (1 << CAP_H) * ((N >> CAP_H) - 2) + (1 << CAP_H)  # internal nodes + cap entries
+    PERMS = LEAF_PERMS + NODE_PERMS
+    LDE_BYTES = 8 * B * (n + N)
+    TRANSPOSE_BYTES = 16 * B * N
+
+
+set_workload()
 
 
 def field_elems(seed: int, count: int) -> np.ndarray:
@@ -172,7 +185,7 @@ def run_reference(args) -> None:
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 (GF(p), p = 2^64 - 2^32 + 1)", "data": "synthetic",
         "config": {"workload": WORKLOAD, "polys": B, "lg_n": LG_N, "rate_bits": RATE, "cap_height": CAP_H,
-                   "hash": "poseidon", "threads": int(os.environ["OMP_NUM_THREADS"])},
+                   "hash": HASH_NAME, "threads": int(os.environ["OMP_NUM_THREADS"])},
         "cpu_baseline": {"value": v, "unit": "elems/s", "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": kind,
                          "sample": sample},
         "e2e": {"value": v, "unit": "elems/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -187,7 +200,13 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--polys", type=int, default=135, help="polynomials (leaf width)")
+    ap.add_argument("--lg-n", type=int, default=15, help="log2 coefficients per polynomial")
+    ap.add_argument("--rate-bits", type=int, default=3)
+    ap.add_argument("--cap-height", type=int, default=4)
+    ap.add_argument("--hash", default="poseidon", choices=sorted(HASH_NAMES))
     args = ap.parse_args()
+    set_workload(args.polys, args.lg_n, args.rate_bits, args.cap_height, args.hash)
     if args.impl == "reference":
         run_reference(args)
         return
@@ -302,15 +321,15 @@ def main() -> None:
         peaks = measured_peaks()
         hbm_peak = peaks.get("hbm_gbs")
         int_peak = int32_peak()
-        ops = PERMS * POSEIDON_OPS
+        ops = PERMS * OPS_PER_PERM[HASH]
         roof = {
-            "kernel": "Merkle build (leaf sponge + levels + cap), Poseidon",
+            "kernel": f"Merkle build (leaf sponge + levels + cap), {HASH_NAME}",
             "bound": "int32", "unit": "Gop/s",
             "achieved": ops / (t_mk * 1e-3) / 1e9,
             "peak": int_peak / 1e9 if int_peak else None,
             "frac": (ops / (t_mk * 1e-3)) / int_peak if int_peak else None,
             "traffic": None,
-            "work_per_launch": f"{PERMS} Poseidon permutations x {POSEIDON_OPS} INT32 multiply-class ops",
+            "work_per_launch": f"{PERMS} {HASH_NAME} permutations x {OPS_PER_PERM[HASH]} INT32 multiply-class ops",
             "peak_source": "INT32 IMAD issue rate measured live by zeknox_b200/libzkprobe.so (MEASURED_PEAKS.json "
                            "has no integer figure)",
             "ms_per_launch": t_mk,
@@ -329,7 +348,7 @@ def main() -> None:
             "scaling": "weak", "vs_baseline": None, "dtype": "u64 (GF(p), p = 2^64 - 2^32 + 1)",
             "data": "synthetic (SplitMix64 seeded, uniform in [0,p))",
             "config": {"workload": WORKLOAD, "polys": B, "lg_n": LG_N, "rate_bits": RATE, "cap_height": CAP_H,
-                       "hash": "poseidon", "parallelism": f"replicas x{world}",
+                       "hash": HASH_NAME, "parallelism": f"replicas x{world}",
                        "l2": f"inputs rotated over {N_ROT} buffers ({N_ROT * B * n * 8 >> 20} MiB > L2); per-step "
                              f"working set {(B * n + 2 * B * N + 4 * nd) * 8 >> 20} MiB"},
             "e2e": {"value": e2e_val, "unit": "elems/s", "h2d_bytes_per_step": B * n * 8,

@@ -127,3 +127,100 @@ __device__ __forceinline__ uint64_t gl_pow7(uint64_t x) {
 __device__ __forceinline__ uint64_t gl_canon(uint64_t x) { return x >= ZK_P ? x - ZK_P : x; }
 
 }  // namespace zk
+
+// ---------------------------------------------------------------------------
+// Partially reduced arithmetic for the hash permutations: a value is any u64
+// congruent to the field element (so in [0, 2^64), not necessarily < p).
+// Results are exact modulo p; callers canonicalise (gl_canon) before storing.
+// ---------------------------------------------------------------------------
+namespace zk {
+
+// (h1, h0, l1, l0) 128-bit -> u64 congruent mod p:
+//   x = (l1:l0) - h1 + h0 * (2^32 - 1).
+__device__ __forceinline__ uint64_t pr_reduce128(uint32_t l0, uint32_t l1, uint32_t h0, uint32_t h1) {
+    uint32_t r0, r1;
+    asm("{\n\t"
+        ".reg .u32 b, k;\n\t"
+        "sub.cc.u32  %0, %2, %5;\n\t"   // r = (l1:l0) - h1
+        "subc.cc.u32 %1, %3, 0;\n\t"
+        "subc.u32    b, 0, 0;\n\t"      // b = all-ones on borrow
+        "sub.cc.u32  %0, %0, b;\n\t"    // on borrow: r -= EPS (r + p mod 2^64)
+        "subc.u32    %1, %1, 0;\n\t"
+        "add.cc.u32  %1, %1, %4;\n\t"   // r += h0 * 2^32
+        "addc.u32    k, 0, 0;\n\t"
+        "sub.cc.u32  %0, %0, %4;\n\t"   // r -= h0
+        "subc.cc.u32 %1, %1, 0;\n\t"
+        "subc.u32    k, k, 0;\n\t"      // k = 1 iff r + h0*EPS overflowed 2^64
+        "neg.s32     k, k;\n\t"
+        "add.cc.u32  %0, %0, k;\n\t"    // then add 2^64 mod p = EPS
+        "addc.u32    %1, %1, 0;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"(l0), "r"(l1), "r"(h0), "r"(h1));
+    return ((uint64_t)r1 << 32) | r0;
+}
+
+// a * b for any u64 a, b; result partially reduced.
+__device__ __forceinline__ uint64_t pr_mul(uint64_t a, uint64_t b) {
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    const uint64_t p00 = (uint64_t)a0 * b0;
+    const uint64_t t = (uint64_t)a0 * b1 + (p00 >> 32);
+    const uint64_t u = (uint64_t)a1 * b0 + (uint32_t)t;
+    const uint64_t v = (uint64_t)a1 * b1 + (t >> 32) + (u >> 32);  // <= 2^64 - 1
+    return pr_reduce128((uint32_t)p00, (uint32_t)u, (uint32_t)v, (uint32_t)(v >> 32));
+}
+
+// a * b + c (a, b any u64; c < 2^68 given as (c_lo, c_hi)); partially reduced.
+__device__ __forceinline__ uint64_t pr_mul_add(uint64_t a, uint64_t b, uint64_t c_lo, uint32_t c_hi) {
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    const uint64_t p00 = (uint64_t)a0 * b0;
+    const uint64_t t = (uint64_t)a0 * b1 + (p00 >> 32);
+    const uint64_t u = (uint64_t)a1 * b0 + (uint32_t)t;
+    uint64_t v = (uint64_t)a1 * b1 + (t >> 32) + (u >> 32);
+    const uint64_t lo = ((uint64_t)(uint32_t)u << 32) | (uint32_t)p00;
+    // (v:lo) + (c_hi:c_lo) <= (2^64-1)^2 + 2^68 < 2^128
+    const uint64_t s = lo + c_lo;
+    v += (uint64_t)c_hi + (s < lo ? 1u : 0u);
+    return pr_reduce128((uint32_t)s, (uint32_t)(s >> 32), (uint32_t)v, (uint32_t)(v >> 32));
+}
+
+// a + c for any u64 a and c < p: one wrap at most, fixed by adding EPS.
+__device__ __forceinline__ uint64_t pr_add_c(uint64_t a, uint64_t c) {
+    const uint64_t s = a + c;
+    return s < a ? s + ZK_EPS : s;
+}
+
+// x^7 with partial reduction (2 squarings, 2 products).
+__device__ __forceinline__ uint64_t pr_pow7(uint64_t x) {
+    const uint64_t x2 = pr_mul(x, x);
+    const uint64_t x3 = pr_mul(x, x2);
+    const uint64_t x4 = pr_mul(x2, x2);
+    return pr_mul(x3, x4);
+}
+
+// al + ah * 2^32 + c for al, ah < 2^60 and any c < 2^64; partially reduced.
+__device__ __forceinline__ uint64_t pr_reduce_split(uint64_t al, uint64_t ah, uint64_t c) {
+    uint32_t r0, r1;
+    asm("{\n\t"
+        ".reg .u32 k, j;\n\t"
+        "add.cc.u32  %0, %2, %6;\n\t"   // r = al + c
+        "addc.cc.u32 %1, %3, %7;\n\t"
+        "addc.u32    k, 0, 0;\n\t"
+        "add.cc.u32  %1, %1, %4;\n\t"   // r += lo32(ah) * 2^32
+        "addc.u32    k, k, %5;\n\t"     // k = 2^64 carries + hi32(ah)
+        "add.cc.u32  %1, %1, k;\n\t"    // r += k * EPS = k * 2^32 - k
+        "addc.u32    j, 0, 0;\n\t"
+        "sub.cc.u32  %0, %0, k;\n\t"
+        "subc.cc.u32 %1, %1, 0;\n\t"
+        "subc.u32    j, j, 0;\n\t"      // j = 1 iff that overflowed 2^64
+        "neg.s32     j, j;\n\t"
+        "add.cc.u32  %0, %0, j;\n\t"
+        "addc.u32    %1, %1, 0;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"((uint32_t)al), "r"((uint32_t)(al >> 32)), "r"((uint32_t)ah), "r"((uint32_t)(ah >> 32)),
+          "r"((uint32_t)c), "r"((uint32_t)(c >> 32)));
+    return ((uint64_t)r1 << 32) | r0;
+}
+
+}  // namespace zk

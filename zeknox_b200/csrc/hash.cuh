@@ -23,12 +23,14 @@ __constant__ uint64_t c_poseidon2_rc[360] = {ZK_POSEIDON2_RC_LIST};
 __constant__ uint64_t c_poseidon2_diag[12] = {ZK_POSEIDON2_DIAG_LIST};
 __constant__ uint64_t c_keccak_rc[24] = {ZK_KECCAK_RC_LIST};
 
-// out = M * x for a 12x12 matrix of small non-negative integer coefficients
-// (row sums < 2^9), computed on the 32-bit halves of x with 64-bit
-// accumulators and reduced once per row.  coef(r, c) must be a constant
-// expression after unrolling.
+// out = M * x (+ c) for a 12x12 matrix of small non-negative integer
+// coefficients (row sums < 2^9): multiply-accumulate on the 32-bit halves of
+// x into 64-bit accumulators (one IMAD.WIDE per term and half), then one
+// partial reduction per row, which also adds c[r] (the next round's
+// constants; c == nullptr adds nothing).  Inputs and outputs are partially
+// reduced.  coef(r, c) must be a constant expression after unrolling.
 template <class Coef>
-__device__ __forceinline__ void small_matvec12(uint64_t s[12], Coef coef) {
+__device__ __forceinline__ void small_matvec12(uint64_t s[12], Coef coef, const uint64_t *c) {
     uint32_t lo[12], hi[12];
 #pragma unroll
     for (int i = 0; i < 12; i++) {
@@ -39,17 +41,14 @@ __device__ __forceinline__ void small_matvec12(uint64_t s[12], Coef coef) {
     for (int r = 0; r < 12; r++) {
         uint64_t al = 0, ah = 0;
 #pragma unroll
-        for (int c = 0; c < 12; c++) {
-            const uint32_t k = coef(r, c);
-            if (k) {
-                al += (uint64_t)k * lo[c];
-                ah += (uint64_t)k * hi[c];
+        for (int k = 0; k < 12; k++) {
+            const uint32_t m = coef(r, k);
+            if (m) {
+                al += (uint64_t)m * lo[k];
+                ah += (uint64_t)m * hi[k];
             }
         }
-        // value = al + ah * 2^32 < 2^74
-        uint64_t l64 = al + (ah << 32);
-        uint32_t h32 = (uint32_t)(ah >> 32) + (l64 < al ? 1u : 0u);
-        s[r] = gl_reduce96(l64, h32);
+        s[r] = pr_reduce_split(al, ah, c ? c[r] : 0ull);
     }
 }
 
@@ -62,25 +61,35 @@ struct PoseidonMds {
     }
 };
 
+// x^7 on all 12 lanes, as three passes over 4 lanes with a rotation between
+// them (keeps the loop body, and so the instruction footprint, small).
+__device__ __forceinline__ void pow7_all(uint64_t s[12]) {
+#pragma unroll 1
+    for (int q = 0; q < 3; q++) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) s[i] = pr_pow7(s[i]);
+        const uint64_t t0 = s[0], t1 = s[1], t2 = s[2], t3 = s[3];
+#pragma unroll
+        for (int i = 0; i < 8; i++) s[i] = s[i + 4];
+        s[8] = t0;
+        s[9] = t1;
+        s[10] = t2;
+        s[11] = t3;
+    }
+}
+
+// The permutation on a partially reduced state (outputs partially reduced).
+// Round r adds its 12 constants, applies x^7 (all lanes in rounds 0-3 and
+// 26-29, lane 0 otherwise) and the MDS layer; each round's constants are
+// added inside the previous round's MDS reduction.
 __device__ __forceinline__ void poseidon_permute(uint64_t s[12]) {
 #pragma unroll
-    for (int rnd = 0; rnd < 4; rnd++) {
-#pragma unroll
-        for (int i = 0; i < 12; i++) s[i] = gl_pow7(gl_add(s[i], c_poseidon_rc[12 * rnd + i]));
-        small_matvec12(s, PoseidonMds());
-    }
+    for (int i = 0; i < 12; i++) s[i] = pr_add_c(s[i], c_poseidon_rc[i]);
 #pragma unroll 1
-    for (int rnd = 4; rnd < 26; rnd++) {
-#pragma unroll
-        for (int i = 0; i < 12; i++) s[i] = gl_add(s[i], c_poseidon_rc[12 * rnd + i]);
-        s[0] = gl_pow7(s[0]);
-        small_matvec12(s, PoseidonMds());
-    }
-#pragma unroll
-    for (int rnd = 26; rnd < 30; rnd++) {
-#pragma unroll
-        for (int i = 0; i < 12; i++) s[i] = gl_pow7(gl_add(s[i], c_poseidon_rc[12 * rnd + i]));
-        small_matvec12(s, PoseidonMds());
+    for (int rnd = 0; rnd < 30; rnd++) {
+        if (rnd < 4 || rnd >= 26) pow7_all(s);
+        else s[0] = pr_pow7(s[0]);
+        small_matvec12(s, PoseidonMds(), rnd < 29 ? &c_poseidon_rc[12 * (rnd + 1)] : nullptr);
     }
 }
 
@@ -94,33 +103,41 @@ struct Poseidon2External {
     }
 };
 
-__device__ __forceinline__ void poseidon2_internal(uint64_t s[12]) {
-    // x_i <- x_i * D_i + sum_j x_j   (poseidon2.cu:131-146)
-    uint64_t sum = s[0];
+// x_i <- x_i * D_i + sum_j x_j (+ next round's constants): poseidon2.cu:131-146.
+__device__ __forceinline__ void poseidon2_internal(uint64_t s[12], const uint64_t *c) {
+    uint64_t sl = s[0];
+    uint32_t sh = 0;
 #pragma unroll
-    for (int i = 1; i < 12; i++) sum = gl_add(sum, s[i]);
+    for (int i = 1; i < 12; i++) {
+        const uint64_t t = sl + s[i];
+        sh += t < sl ? 1u : 0u;
+        sl = t;
+    }
 #pragma unroll
-    for (int i = 0; i < 12; i++) s[i] = gl_add(gl_mul(s[i], c_poseidon2_diag[i]), sum);
+    for (int i = 0; i < 12; i++) {
+        const uint64_t cl = sl + c[i];
+        const uint32_t ch = sh + (cl < sl ? 1u : 0u);
+        s[i] = pr_mul_add(s[i], c_poseidon2_diag[i], cl, ch);
+    }
 }
 
 __device__ __forceinline__ void poseidon2_permute(uint64_t s[12]) {
-    small_matvec12(s, Poseidon2External());
-#pragma unroll
+    small_matvec12(s, Poseidon2External(), &c_poseidon2_rc[0]);
+#pragma unroll 1
     for (int rnd = 0; rnd < 4; rnd++) {
-#pragma unroll
-        for (int i = 0; i < 12; i++) s[i] = gl_pow7(gl_add(s[i], c_poseidon2_rc[12 * rnd + i]));
-        small_matvec12(s, Poseidon2External());
+        pow7_all(s);
+        small_matvec12(s, Poseidon2External(), &c_poseidon2_rc[12 * (rnd + 1)]);
     }
+    // internal rounds: only lane 0 of their constants is non-zero
 #pragma unroll 1
     for (int rnd = 4; rnd < 26; rnd++) {
-        s[0] = gl_pow7(gl_add(s[0], c_poseidon2_rc[12 * rnd]));
-        poseidon2_internal(s);
+        s[0] = pr_pow7(s[0]);
+        poseidon2_internal(s, &c_poseidon2_rc[12 * (rnd + 1)]);
     }
-#pragma unroll
+#pragma unroll 1
     for (int rnd = 26; rnd < 30; rnd++) {
-#pragma unroll
-        for (int i = 0; i < 12; i++) s[i] = gl_pow7(gl_add(s[i], c_poseidon2_rc[12 * rnd + i]));
-        small_matvec12(s, Poseidon2External());
+        pow7_all(s);
+        small_matvec12(s, Poseidon2External(), rnd < 29 ? &c_poseidon2_rc[12 * (rnd + 1)] : nullptr);
     }
 }
 
@@ -164,7 +181,9 @@ template <int H>
 __device__ __forceinline__ void hash_one(const uint64_t *__restrict__ in, uint32_t n, uint64_t *__restrict__ out) {
     if constexpr (H == kKeccak) {
         if (n < 4) {  // copy n words, leave the rest of the digest as it was
-            for (uint32_t i = 0; i < n; i++) out[i] = in[i];
+#pragma unroll
+            for (uint32_t i = 0; i < 4; i++)
+                if (i < n) out[i] = in[i];
             return;
         }
         uint64_t a[25];
@@ -191,9 +210,8 @@ __device__ __forceinline__ void hash_one(const uint64_t *__restrict__ in, uint32
         out[3] = a[3] & 0xffull;
     } else {
         if (n <= 4) {
-            uint32_t i = 0;
-            for (; i < n; i++) out[i] = in[i];
-            for (; i < 4; i++) out[i] = 0;
+#pragma unroll
+            for (uint32_t i = 0; i < 4; i++) out[i] = i < n ? in[i] : 0ull;
             return;
         }
         uint64_t s[12];
@@ -212,10 +230,10 @@ __device__ __forceinline__ void hash_one(const uint64_t *__restrict__ in, uint32
             if constexpr (H == kPoseidon) poseidon_permute(s);
             else poseidon2_permute(s);
         }
-        out[0] = s[0];
-        out[1] = s[1];
-        out[2] = s[2];
-        out[3] = s[3];
+        out[0] = gl_canon(s[0]);
+        out[1] = gl_canon(s[1]);
+        out[2] = gl_canon(s[2]);
+        out[3] = gl_canon(s[3]);
     }
 }
 
@@ -250,10 +268,10 @@ __device__ __forceinline__ void hash_two(const uint64_t *l, const uint64_t *r, u
         }
         if constexpr (H == kPoseidon) poseidon_permute(s);
         else poseidon2_permute(s);
-        out[0] = s[0];
-        out[1] = s[1];
-        out[2] = s[2];
-        out[3] = s[3];
+        out[0] = gl_canon(s[0]);
+        out[1] = gl_canon(s[1]);
+        out[2] = gl_canon(s[2]);
+        out[3] = gl_canon(s[3]);
     }
 }
 

@@ -1,12 +1,19 @@
 // Merkle forest construction in zeknox's linear digest layout
 // (native/merkle/merkle.cu:166-244).
 //
-// Leaf hashing runs one thread per leaf with the sponge state in registers
-// (kernel `merkle_leaves`).  The internal levels of all 2^cap_height subtrees
-// are built bottom-up; `merkle_tile_levels` folds the lowest levels inside a
-// thread block (shared memory, no extra launches) and `merkle_level` handles
-// the remaining wide levels; `merkle_caps` hashes the subtree roots.
+// zeknox launches one kernel for the leaves, one per tree level and one for
+// the cap (merkle.cu:215-243).  Here `merkle_tile` gives each block a tile of
+// 128 consecutive leaves of one subtree: every thread runs its leaf's sponge
+// with the state in registers, then the block folds the tile's 7 lowest
+// levels through shared memory, writing every digest on the way.  The levels
+// above the tiles (fewer than 2^cap_height * L/128 nodes) are finished by
+// `merkle_top`, one block per subtree, which also writes the cap.  The
+// special shapes (cap == leaves, 1 or 2 leaves per subtree, Keccak leaves
+// shorter than a digest) use the one-thread-per-hash kernels
+// `merkle_leaves` / `merkle_caps`.
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "hash.cuh"
 #include "merkle.cuh"
@@ -51,6 +58,70 @@ __global__ void __launch_bounds__(kLeafThreads) merkle_level(uint64_t *__restric
     hash_two<H>(base + 4 * (2 * i + 2), base + 4 * (2 * i + 3), base + 4 * i);
 }
 
+constexpr int kTile = 128;
+
+// Level of width w (nodes per subtree) starts at offset w - 2 of the subtree's
+// digest block; width 1 is the subtree root, which is the cap entry.
+__device__ __forceinline__ uint64_t *node_ptr(uint64_t *sub, uint64_t w, uint64_t i) { return sub + 4 * (w - 2 + i); }
+
+// Block = tile of blockDim.x (<= 128, a power of two) consecutive leaves of one
+// subtree.  Hashes the leaves, then folds log2(blockDim.x) levels.
+template <int H>
+__global__ void __launch_bounds__(kTile) merkle_tile(const uint64_t *__restrict__ leaves, uint32_t leaf_size,
+                                                     uint64_t *__restrict__ digests, uint64_t *__restrict__ cap,
+                                                     uint64_t ls, uint64_t ds) {
+    __shared__ uint64_t sm[kTile * 4];
+    const uint32_t t = threadIdx.x, T = blockDim.x;
+    const uint64_t leaf = blockIdx.x * (uint64_t)T + t;
+    const uint64_t sub = leaf / ls, j0 = (blockIdx.x * (uint64_t)T) % ls;
+    uint64_t *base = digests + 4 * sub * ds;
+    uint64_t d[4];
+    hash_one<H>(leaves + leaf * leaf_size, leaf_size, d);
+    uint64_t *dst = base + 4 * (ds - ls + j0 + t);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        dst[k] = d[k];
+        sm[4 * t + k] = d[k];
+    }
+    uint64_t w = ls;
+    for (uint32_t active = T >> 1; active >= 1; active >>= 1) {
+        w >>= 1;
+        __syncthreads();
+        uint64_t h[4];
+        if (t < active) hash_two<H>(&sm[8 * t], &sm[8 * t + 4], h);
+        __syncthreads();
+        if (t < active) {
+            const uint64_t i = (j0 >> (__ffs(T / active) - 1)) + t;  // index in the level of width w
+            uint64_t *o = w >= 2 ? node_ptr(base, w, i) : cap + 4 * sub;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                o[k] = h[k];
+                sm[4 * t + k] = h[k];
+            }
+        }
+    }
+}
+
+// One block per subtree: the levels above the tiles, from width w0 down to the
+// root (written to cap[sub]).
+template <int H>
+__global__ void __launch_bounds__(256) merkle_top(uint64_t *__restrict__ digests, uint64_t *__restrict__ cap,
+                                                  uint64_t ds, uint64_t w0) {
+    const uint64_t sub = blockIdx.x;
+    uint64_t *base = digests + 4 * sub * ds;
+    for (uint64_t w = w0; w > 1; w >>= 1) {
+        const uint64_t wn = w >> 1;
+        for (uint64_t i = threadIdx.x; i < wn; i += blockDim.x) {
+            uint64_t h[4];
+            hash_two<H>(node_ptr(base, w, 2 * i), node_ptr(base, w, 2 * i + 1), h);
+            uint64_t *o = wn >= 2 ? node_ptr(base, wn, i) : cap + 4 * sub;
+#pragma unroll
+            for (int k = 0; k < 4; k++) o[k] = h[k];
+        }
+        __syncthreads();
+    }
+}
+
 template <int H>
 __global__ void merkle_caps(uint64_t *__restrict__ cap, const uint64_t *__restrict__ digests, uint64_t n_caps,
                             uint64_t ds) {
@@ -82,19 +153,33 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
         ZK_CHECK_LAUNCH();
         return;
     }
-    LeafMap map;
-    map.direct = (ls == 2);
-    map.ls = ls;
-    map.ds = ds;
-    merkle_leaves<H><<<blocks_for(j.n_leaves, kLeafThreads), kLeafThreads, 0, st>>>(j.leaves, j.n_leaves, w, j.digests,
-                                                                                     map);
+    if (ls == 2 || (H == kKeccak && w < 4)) {
+        // zeknox's one-thread-per-hash structure (merkle.cu:193-243); Keccak
+        // leaves shorter than a digest keep the words they do not write.
+        LeafMap map;
+        map.direct = (ls == 2);
+        map.ls = ls;
+        map.ds = ds;
+        merkle_leaves<H><<<blocks_for(j.n_leaves, kLeafThreads), kLeafThreads, 0, st>>>(j.leaves, j.n_leaves, w,
+                                                                                         j.digests, map);
+        ZK_CHECK_LAUNCH();
+        for (uint64_t lw = ls / 2; lw >= 2; lw /= 2) {
+            merkle_level<H><<<blocks_for(lw * j.n_caps, kLeafThreads), kLeafThreads, 0, st>>>(j.digests, lw, j.n_caps,
+                                                                                              ds);
+            ZK_CHECK_LAUNCH();
+        }
+        merkle_caps<H><<<blocks_for(j.n_caps, 64), 64, 0, st>>>(j.cap, j.digests, j.n_caps, ds);
+        ZK_CHECK_LAUNCH();
+        return;
+    }
+    const uint32_t T = (uint32_t)std::min<uint64_t>(kTile, ls);
+    merkle_tile<H><<<blocks_for(j.n_leaves, T), T, 0, st>>>(j.leaves, w, j.digests, j.cap, ls, ds);
     ZK_CHECK_LAUNCH();
-    for (uint64_t lw = ls / 2; lw >= 2; lw /= 2) {
-        merkle_level<H><<<blocks_for(lw * j.n_caps, kLeafThreads), kLeafThreads, 0, st>>>(j.digests, lw, j.n_caps, ds);
+    if (ls > (uint64_t)kTile) {
+        require(j.n_caps < (1ull << 31), "too many subtrees");
+        merkle_top<H><<<(unsigned)j.n_caps, 256, 0, st>>>(j.digests, j.cap, ds, ls / kTile);
         ZK_CHECK_LAUNCH();
     }
-    merkle_caps<H><<<blocks_for(j.n_caps, 64), 64, 0, st>>>(j.cap, j.digests, j.n_caps, ds);
-    ZK_CHECK_LAUNCH();
 }
 
 }  // namespace
