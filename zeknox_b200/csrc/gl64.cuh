@@ -13,6 +13,8 @@
 
 namespace zk {
 
+__device__ __forceinline__ uint64_t gl_canon_fwd(uint64_t x) { return x >= ZK_P ? x - ZK_P : x; }
+
 // a + b mod p for a, b < p.  With s = a + b (mod 2^64) the result is s + EPS
 // (mod 2^64) exactly when the sum carried out or s >= p (i.e. s + EPS carries).
 __device__ __forceinline__ uint64_t gl_add(uint64_t a, uint64_t b) {
@@ -92,11 +94,11 @@ __device__ __forceinline__ void mul_wide(uint64_t a, uint64_t b, uint64_t &lo, u
     hi = ((uint64_t)r3 << 32) | r2;
 }
 
-__device__ __forceinline__ uint64_t gl_mul(uint64_t a, uint64_t b) {
-    uint64_t lo, hi;
-    mul_wide(a, b, lo, hi);
-    return gl_reduce128(lo, hi);
-}
+__device__ __forceinline__ uint64_t pr_mul(uint64_t a, uint64_t b);
+
+// Canonical product: the partially reduced product (below) then one
+// conditional subtraction.
+__device__ __forceinline__ uint64_t gl_mul(uint64_t a, uint64_t b) { return gl_canon_fwd(pr_mul(a, b)); }
 
 __device__ __forceinline__ uint64_t gl_sqr(uint64_t a) { return gl_mul(a, a); }
 
@@ -160,14 +162,13 @@ __device__ __forceinline__ uint64_t pr_reduce128(uint32_t l0, uint32_t l1, uint3
     return ((uint64_t)r1 << 32) | r0;
 }
 
-// a * b for any u64 a, b; result partially reduced.
+// a * b for any u64 a, b; result partially reduced.  The 128-bit product
+// comes from the 32-bit multiply-add chain of mul_wide (cheaper here than
+// 64-bit-accumulating wide multiplies).
 __device__ __forceinline__ uint64_t pr_mul(uint64_t a, uint64_t b) {
-    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
-    const uint64_t p00 = (uint64_t)a0 * b0;
-    const uint64_t t = (uint64_t)a0 * b1 + (p00 >> 32);
-    const uint64_t u = (uint64_t)a1 * b0 + (uint32_t)t;
-    const uint64_t v = (uint64_t)a1 * b1 + (t >> 32) + (u >> 32);  // <= 2^64 - 1
-    return pr_reduce128((uint32_t)p00, (uint32_t)u, (uint32_t)v, (uint32_t)(v >> 32));
+    uint64_t lo, hi;
+    mul_wide(a, b, lo, hi);
+    return pr_reduce128((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
 }
 
 // a * b + c (a, b any u64; c < 2^68 given as (c_lo, c_hi)); partially reduced.

@@ -24,31 +24,34 @@ __constant__ uint64_t c_poseidon2_diag[12] = {ZK_POSEIDON2_DIAG_LIST};
 __constant__ uint64_t c_keccak_rc[24] = {ZK_KECCAK_RC_LIST};
 
 // out = M * x (+ c) for a 12x12 matrix of small non-negative integer
-// coefficients (row sums < 2^9): multiply-accumulate on the 32-bit halves of
-// x into 64-bit accumulators (one IMAD.WIDE per term and half), then one
-// partial reduction per row, which also adds c[r] (the next round's
-// constants; c == nullptr adds nothing).  Inputs and outputs are partially
-// reduced.  coef(r, c) must be a constant expression after unrolling.
+// coefficients (row sums < 2^9).  The 32-bit halves of x are converted to
+// doubles and each row is accumulated with FP64 multiply-adds: every product
+// and partial sum is an integer below 276 * 2^32 < 2^41 < 2^53, so the FP64
+// arithmetic is exact.  This moves the 288 multiply-adds of a layer onto the
+// FP64 pipe (full rate on sm_100), next to the integer pipes that carry the
+// S-box products.  Each row is then reduced once, adding c[r] (the next
+// round's constants; c == nullptr adds nothing).  Inputs and outputs are
+// partially reduced.  coef(r, c) must be a constant expression after unrolling.
 template <class Coef>
 __device__ __forceinline__ void small_matvec12(uint64_t s[12], Coef coef, const uint64_t *c) {
-    uint32_t lo[12], hi[12];
+    double lo[12], hi[12];
 #pragma unroll
     for (int i = 0; i < 12; i++) {
-        lo[i] = (uint32_t)s[i];
-        hi[i] = (uint32_t)(s[i] >> 32);
+        lo[i] = __uint2double_rn((uint32_t)s[i]);
+        hi[i] = __uint2double_rn((uint32_t)(s[i] >> 32));
     }
 #pragma unroll
     for (int r = 0; r < 12; r++) {
-        uint64_t al = 0, ah = 0;
+        double al = 0.0, ah = 0.0;
 #pragma unroll
         for (int k = 0; k < 12; k++) {
             const uint32_t m = coef(r, k);
             if (m) {
-                al += (uint64_t)m * lo[k];
-                ah += (uint64_t)m * hi[k];
+                al = fma((double)m, lo[k], al);
+                ah = fma((double)m, hi[k], ah);
             }
         }
-        s[r] = pr_reduce_split(al, ah, c ? c[r] : 0ull);
+        s[r] = pr_reduce_split(__double2ull_rz(al), __double2ull_rz(ah), c ? c[r] : 0ull);
     }
 }
 

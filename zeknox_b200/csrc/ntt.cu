@@ -56,7 +56,7 @@ struct PassArgs {
     // twiddles
     const uint64_t *tw_lo, *tw_hi;  // omega_N powers (two-level)
     uint32_t tw_h;
-    const uint64_t *line_roots;     // omega_4096^j, j < 2048
+    const uint64_t *line_roots;     // omega_4096^j, j < 4096
 };
 
 __device__ __forceinline__ uint64_t pow2l(const uint64_t *lo, const uint64_t *hi, uint32_t h, uint64_t e) {
@@ -67,26 +67,81 @@ __device__ __forceinline__ uint32_t brev_bits(uint32_t x, uint32_t bits) {
     return bits ? (__brev(x) >> (32 - bits)) : 0u;
 }
 
-// In-place radix-2 DIF over T interleaved lines of length L in shared memory
-// (element e of line t at e * tp + t).  Natural order in, bit-reversed out.
-__device__ __forceinline__ void smem_dif(uint64_t *sm, const uint64_t *tw, uint32_t l, uint32_t T, uint32_t tp) {
-    const uint32_t L = 1u << l;
-    const uint32_t nb = (T * L) >> 1;
-    for (int s = (int)l - 1; s >= 0; s--) {
+// DIF butterfly (u, v) -> (u + v, (u - v) w).
+__device__ __forceinline__ void bfly(uint64_t &u, uint64_t &v, uint64_t w) {
+    const uint64_t d = gl_sub(u, v);
+    u = gl_add(u, v);
+    v = gl_mul(d, w);
+}
+__device__ __forceinline__ void bfly1(uint64_t &u, uint64_t &v) {  // w = 1
+    const uint64_t d = gl_sub(u, v);
+    u = gl_add(u, v);
+    v = d;
+}
+
+// In-place DIF stages over T interleaved lines of length L = 2^l in shared
+// memory (element e of line t at e * tp + t), from half-span 2^s_top down to
+// 1: natural order in, bit-reversed out.  Stages are taken three at a time
+// (radix 8 in registers: one shared-memory round trip per three stages), then
+// a radix-4 or radix-2 tail.  tw[e] = omega_L^e for e < L.
+__device__ __forceinline__ void smem_dif(uint64_t *sm, const uint64_t *tw, uint32_t l, int s_top, uint32_t lg_t,
+                                         uint32_t tp) {
+    const uint32_t T = 1u << lg_t;
+    int s = s_top;
+    while (s >= 2) {  // spans 4q, 2q, q with q = 2^(s-2); unit = 8 elements at stride q
         __syncthreads();
-        const uint32_t h = 1u << s;
-        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {
-            const uint32_t t = b % T, j = b / T;
-            const uint32_t o = j & (h - 1);
-            const uint32_t e0 = ((j >> s) << (s + 1)) + o;
-            const uint32_t i0 = e0 * tp + t, i1 = (e0 + h) * tp + t;
-            const uint64_t u = sm[i0], v = sm[i1];
-            sm[i0] = gl_add(u, v);
-            const uint64_t d = gl_sub(u, v);
-            sm[i1] = o ? gl_mul(d, tw[o << (l - 1 - s)]) : d;
+        const uint32_t lq = s - 2, q = 1u << lq;
+        const uint32_t units = T << (l - 3);
+        const uint32_t sh8 = l - 1 - s;  // omega_{8q}^j = tw[j << sh8]
+        for (uint32_t u = threadIdx.x; u < units; u += blockDim.x) {
+            const uint32_t t = u & (T - 1), w = u >> lg_t;
+            const uint32_t o = w & (q - 1), e0 = ((w >> lq) << (lq + 3)) + o;
+            uint64_t x[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) x[k] = sm[(e0 + k * q) * tp + t];
+#pragma unroll
+            for (int k = 0; k < 4; k++) bfly(x[k], x[k + 4], tw[(o + k * q) << sh8]);
+            const uint64_t w2a = tw[o << (sh8 + 1)], w2b = tw[(o + q) << (sh8 + 1)];
+            bfly(x[0], x[2], w2a);
+            bfly(x[1], x[3], w2b);
+            bfly(x[4], x[6], w2a);
+            bfly(x[5], x[7], w2b);
+            const uint64_t w1 = tw[o << (sh8 + 2)];
+#pragma unroll
+            for (int k = 0; k < 8; k += 2) bfly(x[k], x[k + 1], w1);
+#pragma unroll
+            for (int k = 0; k < 8; k++) sm[(e0 + k * q) * tp + t] = x[k];
         }
+        s -= 3;
     }
     __syncthreads();
+    if (s == 1) {  // spans 2 and 1: radix-4 units
+        const uint32_t units = T << (l - 2);
+        for (uint32_t u = threadIdx.x; u < units; u += blockDim.x) {
+            const uint32_t t = u & (T - 1), e0 = (u >> lg_t) << 2;
+            uint64_t x0 = sm[e0 * tp + t], x1 = sm[(e0 + 1) * tp + t], x2 = sm[(e0 + 2) * tp + t],
+                     x3 = sm[(e0 + 3) * tp + t];
+            bfly1(x0, x2);
+            bfly(x1, x3, tw[(1u << l) >> 2]);  // omega_4
+            bfly1(x0, x1);
+            bfly1(x2, x3);
+            sm[e0 * tp + t] = x0;
+            sm[(e0 + 1) * tp + t] = x1;
+            sm[(e0 + 2) * tp + t] = x2;
+            sm[(e0 + 3) * tp + t] = x3;
+        }
+        __syncthreads();
+    } else if (s == 0) {  // span 1
+        const uint32_t units = T << (l - 1);
+        for (uint32_t u = threadIdx.x; u < units; u += blockDim.x) {
+            const uint32_t t = u & (T - 1), e0 = (u >> lg_t) << 1;
+            uint64_t x0 = sm[e0 * tp + t], x1 = sm[(e0 + 1) * tp + t];
+            bfly1(x0, x1);
+            sm[e0 * tp + t] = x0;
+            sm[(e0 + 1) * tp + t] = x1;
+        }
+        __syncthreads();
+    }
 }
 
 __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
@@ -94,13 +149,10 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
     const uint32_t l = a.l, L = 1u << l;
     const uint32_t T = 1u << a.lg_t;
     const uint32_t tp = T > 1 ? T + 1 : 1;
-    uint64_t *tw = smem;              // L/2 line roots
-    uint64_t *sm = smem + (L >> 1 > 0 ? L >> 1 : 1);
-    // line roots omega_L^j = omega_4096^(j * 4096 / L)
-    for (uint32_t j = threadIdx.x; j < (L >> 1); j += blockDim.x) tw[j] = __ldg(a.line_roots + (j << (kLineLgMax - l)));
-
-    const uint64_t N = 1ull << a.lg_n;
-    uint64_t g = blockIdx.x;
+    uint64_t *tw = smem;  // omega_L^e, e < L
+    uint64_t *sm = smem + L;
+    for (uint32_t j = threadIdx.x; j < L; j += blockDim.x) tw[j] = __ldg(a.line_roots + (j << (kLineLgMax - l)));
+    const uint64_t g = blockIdx.x;
 
     if (a.kind == 0) {
         // ---- column pass: lines r0 + t (t < T) of prefix q, elements at stride S
@@ -115,7 +167,17 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
         const uint64_t base = q << (l + lg_s);  // prefix block start within the polynomial
         const uint64_t *src = a.src + poly * a.src_poly_stride;
         uint64_t *dst = a.dst + poly * a.dst_poly_stride;
-        for (uint32_t idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
+        // Only the first Lv = 2^lv elements of a line can be non-zero (zero
+        // extension): the first l - lv DIF stages then reduce to writing block
+        // b of the line as x_e * omega_L^(e * brev(b)), e < Lv.
+        uint32_t lv = l;
+        if (a.n_valid < ((uint64_t)L << lg_s) && base == 0) {
+            const uint64_t nz = (a.n_valid + S - 1) >> lg_s;  // non-zero prefix of every line
+            lv = nz <= 1 ? 0 : 64 - __clzll(nz - 1);
+        }
+        const uint32_t rr = l - lv;
+        __syncthreads();
+        for (uint32_t idx = threadIdx.x; idx < (T << lv); idx += blockDim.x) {
             const uint32_t t = idx & (T - 1), e = idx >> a.lg_t;
             const uint64_t i = base + ((uint64_t)e << lg_s) + r0 + t;  // index within the polynomial
             uint64_t v = 0;
@@ -124,15 +186,21 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
                 if (a.pre_lo) v = gl_mul(v, pow2l(a.pre_lo, a.pre_hi, a.pre_h, i));
             }
             sm[e * tp + t] = v;
+            for (uint32_t b = 1; b < (1u << rr); b++)
+                sm[((b << lv) + e) * tp + t] = gl_mul(v, tw[(e * brev_bits(b, rr)) & (L - 1)]);
         }
-        __syncthreads();
-        smem_dif(sm, tw, l, T, tp);
-        for (uint32_t idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
-            const uint32_t t = idx & (T - 1), k = idx >> a.lg_t;
-            uint64_t v = sm[brev_bits(k, l) * tp + t];
-            const uint64_t e = ((r0 + t) * (uint64_t)k) << a.lg_pre;  // w_{L S}^{r k} = w_N^{r k Q}
-            if (e) v = gl_mul(v, pow2l(a.tw_lo, a.tw_hi, a.tw_h, e));
-            dst[base + ((uint64_t)k << lg_s) + r0 + t] = v;
+        smem_dif(sm, tw, l, (int)lv - 1, a.lg_t, tp);
+        // store with the inter-pass twiddle w_N^((r0 + t) k Q), stepped by k
+        const uint32_t t = threadIdx.x & (T - 1);
+        const uint32_t k0 = threadIdx.x >> a.lg_t, dk = blockDim.x >> a.lg_t;
+        const uint64_t r = r0 + t;
+        const uint64_t nmask = (1ull << a.lg_n) - 1;  // w_N has order N
+        uint64_t twk = pow2l(a.tw_lo, a.tw_hi, a.tw_h, ((r * k0) << a.lg_pre) & nmask);
+        const uint64_t step = pow2l(a.tw_lo, a.tw_hi, a.tw_h, ((r * dk) << a.lg_pre) & nmask);
+        for (uint32_t k = k0; k < L; k += dk) {
+            const uint64_t v = gl_mul(sm[brev_bits(k, l) * tp + t], twk);
+            dst[base + ((uint64_t)k << lg_s) + r] = v;
+            twk = gl_mul(twk, step);
         }
         return;
     }
@@ -172,8 +240,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
         }
         sm[e * tp + t] = v;
     }
-    __syncthreads();
-    smem_dif(sm, tw, l, T, tp);
+    smem_dif(sm, tw, l, (int)l - 1, a.lg_t, tp);
     if (a.kind == 1) {
         // natural index of line t's element k: krev + Q * k
         uint64_t *dst = a.dst + poly0 * a.dst_poly_stride;
@@ -195,7 +262,6 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
             a.dst[(poly0 + t) * a.dst_poly_stride + k] = v;
         }
     }
-    (void)N;
 }
 
 // out[rev(k) * B + b] = in[b * N + k]: 16 rows x 64 columns per block, through
@@ -265,7 +331,7 @@ uint32_t ilog2_floor(uint64_t x) { return 63 - __builtin_clzll(x); }
 size_t pass_smem(uint32_t l, uint32_t lg_t) {
     const uint64_t T = 1ull << lg_t, tp = T > 1 ? T + 1 : 1;
     const uint64_t L = 1ull << l;
-    return (size_t)(std::max<uint64_t>(L >> 1, 1) + L * tp) * sizeof(uint64_t);
+    return (size_t)(L + L * tp) * sizeof(uint64_t);
 }
 
 void launch_pass(const PassArgs &a, uint64_t groups, cudaStream_t s) {
@@ -386,9 +452,11 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
 uint64_t ntt_scratch_elems(uint32_t lg, uint64_t batches) {
     if (make_plan(lg).passes == 1) return 0;
     const uint64_t N = 1ull << lg;
-    // At most 32 MiB of intermediate (fits in L2 next to the streamed data),
-    // but always at least one polynomial.
-    const uint64_t cap = (32ull << 20) / sizeof(uint64_t);
+    // Intermediate for up to 512 MiB of polynomials per chunk: chunks small
+    // enough to bound the scratch, large enough that each pass launch spans
+    // many waves of blocks (a chunk of a few polynomials leaves most of the
+    // last wave idle).  Always at least one polynomial.
+    const uint64_t cap = (512ull << 20) / sizeof(uint64_t);
     return std::max<uint64_t>(N, std::min<uint64_t>(batches * N, cap / N * N));
 }
 

@@ -98,7 +98,7 @@ const uint64_t *line_roots(DeviceCtx &c, bool inv) {
     if (!c.line_roots[inv]) {
         uint64_t w = h_omega(kLineLgMax);
         if (inv) w = h_inv(w);
-        std::vector<uint64_t> v(1u << (kLineLgMax - 1));
+        std::vector<uint64_t> v(1u << kLineLgMax);
         uint64_t x = 1;
         for (auto &e : v) {
             e = x;
