@@ -149,4 +149,17 @@ ZK_EXTERN RustError zk_merkle_async(void *d_digests, void *d_cap, const void *d_
                                     uint64_t n_caps, uint64_t n_leaves, uint64_t leaf_size, uint64_t cap_height,
                                     uint64_t hash_type, void *stream);
 
+/* Allocation-free coset LDE (no counterpart in zeknox).  Same arguments and
+ * result as zk_lde_async (device buffers, stream-ordered, coset generator 7)
+ * for callers that cannot call cudaMalloc at this point: work captured into a
+ * CUDA graph, provers confined to a pre-reserved memory budget or arena, hot
+ * paths where allocation is forbidden.  Its NTT intermediate and tables live in
+ * one static device array (32 MiB + 96 KiB per GPU, held until exit), so:
+ * lg_n + rate_bits must be <= 22 (else code cudaErrorMemoryAllocation = 2,
+ * NULL message); calls that overlap on the GPU race on the shared array; the
+ * first call on a device resolves the array's address (make it before any
+ * stream capture).  Errors never carry a message (nothing is allocated). */
+ZK_EXTERN RustError zk_lde_noalloc(void *d_output, const void *d_input, uint32_t lg_n, uint32_t rate_bits,
+                                   uint32_t batches, uint32_t inv, uint32_t with_coset, void *stream);
+
 #endif /* ZEKNOX_B200_H */

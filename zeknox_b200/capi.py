@@ -96,6 +96,7 @@ def _load() -> ctypes.CDLL:
         "zk_lde_async": (RustError, [vp, vp, u32, u32, u32, u32, u32, vp]),
         "zk_transpose_rev_async": (RustError, [vp, vp, u32, u32, vp]),
         "zk_merkle_async": (RustError, [vp, vp, vp, u64, u64, u64, u64, u64, u64, vp]),
+        "zk_lde_noalloc": (RustError, [vp, vp, u32, u32, u32, u32, u32, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -477,3 +477,88 @@ void salt_run(uint64_t *out, uint64_t count, uint64_t seed, cudaStream_t s) {
 }
 
 }  // namespace zk
+
+namespace zk {
+
+// The transform of ntt_run, but on tables the caller supplies (no per-device
+// state is created or looked up, so nothing is allocated here): used by the
+// allocation-free LDE entry point in noalloc.cu.
+void ntt_run_on_tables(const NttJob &j, const PowTable &roots, const uint64_t *line_roots_dev, cudaStream_t s) {
+    const uint32_t lg = j.lg;
+    if (j.batches == 0) return;
+    const Plan plan = make_plan(lg);
+    const uint64_t N = 1ull << lg;
+    PassArgs base{};
+    base.lg_n = lg;
+    base.tw_lo = roots.lo();
+    base.tw_hi = roots.hi();
+    base.tw_h = roots.h;
+    base.line_roots = line_roots_dev;
+    base.scale = j.scale;
+    base.batches = j.batches;
+    if (j.pre_coset) {
+        base.pre_lo = j.pre_coset->lo();
+        base.pre_hi = j.pre_coset->hi();
+        base.pre_h = j.pre_coset->h;
+    }
+    if (j.post_coset) {
+        base.post_lo = j.post_coset->lo();
+        base.post_hi = j.post_coset->hi();
+        base.post_h = j.post_coset->h;
+    }
+    if (plan.passes == 1) {
+        PassArgs a = base;
+        a.kind = 2;
+        a.l = lg;
+        a.lg_pre = 0;
+        a.lg_t = std::min<uint32_t>(ilog2_floor(kLinesElems) - lg, 6);
+        a.src = j.src;
+        a.dst = j.dst;
+        a.src_poly_stride = j.src_stride;
+        a.dst_poly_stride = j.dst_stride;
+        a.n_valid = j.n_valid;
+        launch_pass(a, (j.batches + (1ull << a.lg_t) - 1) >> a.lg_t, s);
+        return;
+    }
+    const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(j.batches, j.scratch_elems / N));
+    for (uint64_t b0 = 0; b0 < j.batches; b0 += chunk) {
+        const uint64_t nb = std::min<uint64_t>(chunk, j.batches - b0);
+        uint32_t lg_s = lg;
+        for (int p = 0; p < plan.passes; p++) {
+            PassArgs a = base;
+            a.l = plan.l[p];
+            a.l_first = plan.l[0];
+            a.batches = (uint32_t)nb;
+            if (p < plan.passes - 1) {
+                lg_s -= a.l;
+                a.kind = 0;
+                a.lg_s = lg_s;
+                a.lg_pre = lg - a.l - lg_s;
+                a.lg_t = std::min<uint32_t>(std::min<uint32_t>(ilog2_floor(kLinesElems) - a.l, lg_s), 5);
+                a.src = p == 0 ? j.src + b0 * j.src_stride : j.scratch;
+                a.src_poly_stride = p == 0 ? j.src_stride : N;
+                a.n_valid = p == 0 ? j.n_valid : N;
+                if (p != 0) a.pre_lo = nullptr;
+                a.dst = j.scratch;
+                a.dst_poly_stride = N;
+                a.post_lo = nullptr;
+                a.scale = 1;
+                launch_pass(a, nb << (lg - a.l - a.lg_t), s);
+            } else {
+                a.kind = 1;
+                a.lg_s = 0;
+                a.lg_pre = lg - a.l;
+                a.lg_t = std::min<uint32_t>(std::min<uint32_t>(ilog2_floor(kLinesElems) - a.l, plan.l[0]), 5);
+                a.src = j.scratch;
+                a.src_poly_stride = N;
+                a.dst = j.dst + b0 * j.dst_stride;
+                a.dst_poly_stride = j.dst_stride;
+                a.pre_lo = nullptr;
+                a.n_valid = N;
+                launch_pass(a, nb << (a.lg_pre - a.lg_t), s);
+            }
+        }
+    }
+}
+
+}  // namespace zk

@@ -36,3 +36,10 @@ void transpose_rev_run(uint64_t *out, const uint64_t *in, uint32_t lg_n, uint32_
 void salt_run(uint64_t *out, uint64_t count, uint64_t seed, cudaStream_t s);
 
 }  // namespace zk
+
+namespace zk {
+// ntt_run on caller-supplied tables (roots: powers of omega_N for this
+// direction, two-level; line_roots: omega_4096^j, j < 4096, this direction).
+// Creates no per-device state and allocates nothing.
+void ntt_run_on_tables(const NttJob &job, const PowTable &roots, const uint64_t *line_roots, cudaStream_t s);
+}  // namespace zk
