@@ -145,6 +145,18 @@ ZK_EXTERN RustError zk_lde_async(void *d_output, const void *d_input, uint32_t l
                                  uint32_t batches, uint32_t inv, uint32_t with_coset, void *stream);
 ZK_EXTERN RustError zk_transpose_rev_async(void *d_output, const void *d_input, uint32_t lg_n, uint32_t batches,
                                            void *stream);
+/* Forward coset LDE (generator 7, or the one init_coset installed) written
+ * directly in the leaf layout of compute_transpose_rev: d_leaves[rev(k)][b] =
+ * LDE_b[k], 2^(lg_n+rate_bits) rows of `batches` elements.  Equals
+ * compute_batched_lde followed by compute_transpose_rev, without the
+ * intermediate LDE matrix. */
+ZK_EXTERN RustError zk_lde_leaves_async(void *d_leaves, const void *d_coeffs, uint32_t lg_n, uint32_t rate_bits,
+                                        uint32_t batches, void *stream);
+/* One commit: zk_lde_leaves_async then the Merkle forest over those leaves
+ * (digests 2*(N - 2^cap_height) x 4, cap 2^cap_height x 4, N = 2^(lg_n+rate_bits)). */
+ZK_EXTERN RustError zk_commit_async(const void *d_coeffs, uint32_t lg_n, uint32_t rate_bits, uint32_t batches,
+                                    uint32_t cap_height, uint32_t hash_type, void *d_leaves, void *d_digests,
+                                    void *d_cap, void *stream);
 ZK_EXTERN RustError zk_merkle_async(void *d_digests, void *d_cap, const void *d_leaves, uint64_t n_digests,
                                     uint64_t n_caps, uint64_t n_leaves, uint64_t leaf_size, uint64_t cap_height,
                                     uint64_t hash_type, void *stream);
@@ -161,5 +173,43 @@ ZK_EXTERN RustError zk_merkle_async(void *d_digests, void *d_cap, const void *d_
  * stream capture).  Errors never carry a message (nothing is allocated). */
 ZK_EXTERN RustError zk_lde_noalloc(void *d_output, const void *d_input, uint32_t lg_n, uint32_t rate_bits,
                                    uint32_t batches, uint32_t inv, uint32_t with_coset, void *stream);
+
+/* ---- batched and served commits (no counterpart in zeknox) ---- */
+
+/* One commit job on device buffers: coefficients batches x 2^lg_n; outputs
+ * leaves 2^(lg_n+rate_bits) x batches (leaf layout), digests
+ * 2*(N - 2^cap_height) x 4, cap 2^cap_height x 4. */
+typedef struct {
+    const void *d_coeffs;
+    uint32_t lg_n, rate_bits, batches, cap_height, hash_type;
+    void *d_leaves, *d_digests, *d_cap;
+} ZkCommitJob;
+
+/* All jobs, stream-ordered on `stream`: forked onto n_streams internal streams
+ * (0 = 4), largest jobs first onto the least-loaded stream, joined back.  Each
+ * job's outputs equal zk_commit_async's. */
+ZK_EXTERN RustError zk_commit_batch(const ZkCommitJob *jobs, uint32_t n_jobs, uint32_t n_streams, void *stream);
+
+/* Commit server: jobs are submitted with host coefficients (kept valid by the
+ * caller until the job completes), admitted onto n_slots concurrent streams
+ * while leaves + digests + cap of resident trees plus coefficients + scratch of
+ * running jobs fit hbm_budget_bytes, and keep their tree on the device until
+ * released.  zk_server_wait blocks until the cap is on the host. */
+typedef struct ZkServer ZkServer;
+typedef struct {
+    uint64_t completed, queued, max_queue;
+    double p50_s, p99_s, max_s; /* submit -> cap on the host */
+    double elems, elems_per_s;  /* committed LDE evaluations; first submit -> last completion */
+    uint64_t hbm_in_use, hbm_peak;
+} ZkServerStats;
+ZK_EXTERN RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes, uint32_t n_slots, ZkServer **out);
+ZK_EXTERN RustError zk_server_submit(ZkServer *srv, const void *host_coeffs, uint32_t lg_n, uint32_t rate_bits,
+                                     uint32_t batches, uint32_t cap_height, uint32_t hash_type, uint64_t *ticket);
+ZK_EXTERN RustError zk_server_wait(ZkServer *srv, uint64_t ticket, uint64_t *host_cap, double *latency_s);
+ZK_EXTERN RustError zk_server_result(ZkServer *srv, uint64_t ticket, void **d_leaves, void **d_digests,
+                                     void **d_cap);
+ZK_EXTERN RustError zk_server_release(ZkServer *srv, uint64_t ticket);
+ZK_EXTERN RustError zk_server_stats(ZkServer *srv, ZkServerStats *out);
+ZK_EXTERN RustError zk_server_destroy(ZkServer *srv);
 
 #endif /* ZEKNOX_B200_H */

@@ -1,0 +1,119 @@
+"""GPU parity of the commit-level extensions: the fused LDE -> leaves pass, the
+single commit, the batched commit and the commit server, each bit-exact
+against the drop-in entry points / the oracle, alone and in the mix."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def zk():
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import zeknox_b200 as zk
+
+    zk.init_coset(0, 24, 7)
+    return zk
+
+
+def _dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("lg_n,rate,b", [(4, 1, 3), (9, 3, 17), (10, 2, 135), (12, 3, 33), (15, 3, 135),
+                                         (17, 2, 5), (18, 3, 7), (8, 1, 200)])
+def test_lde_leaves_equals_lde_then_transpose(zk, oracle, lg_n, rate, b):
+    import torch
+
+    x = _dev(oracle.field_elems(300 + lg_n, b << lg_n)).view(b, 1 << lg_n)
+    fused = zk.lde_leaves(x, rate)
+    two_step = zk.transpose_rev(zk.lde(x, rate))
+    torch.cuda.synchronize()
+    assert torch.equal(fused.view(torch.int64), two_step.view(torch.int64))
+
+
+@pytest.mark.parametrize("ht", [0, 3, 1])
+def test_commit_vs_oracle(zk, oracle, ht):
+    import torch
+
+    lg_n, rate, b, ch = 9, 3, 135, 4
+    x = oracle.field_elems(55 + ht, b << lg_n)
+    out = zk.commit(_dev(x).view(b, 1 << lg_n), rate, ch, ht)
+    torch.cuda.synchronize()
+    leaves = oracle.transpose_rev(oracle.batch_lde(x, lg_n, rate, b), lg_n + rate, b)
+    d, c = oracle.merkle_fill(leaves, b, ch, ht)
+    assert np.array_equal(out.leaves.cpu().numpy().reshape(-1), leaves)
+    assert np.array_equal(out.digests.cpu().numpy().reshape(-1), d)
+    assert np.array_equal(out.cap.cpu().numpy().reshape(-1), c)
+
+
+def _mixed_jobs(oracle, n_jobs, seed):
+    """Shapes drawn like the batched workload (log size, width, rate), scaled down."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(n_jobs):
+        lg_n = int(rng.integers(4, 13))
+        b = int(rng.integers(4, 201))
+        rate = int(rng.integers(1, 4))
+        ch = int(min(4, lg_n + rate - 1))
+        ht = [0, 3, 1][i % 3]
+        jobs.append((oracle.field_elems(seed * 1000 + i, b << lg_n).reshape(b, 1 << lg_n), rate, ch, ht))
+    return jobs
+
+
+def test_commit_batch_equals_individual_commits(zk, oracle):
+    import torch
+
+    jobs = _mixed_jobs(oracle, 24, 7)
+    alone, batch = [], []
+    for x, r, ch, ht in jobs:
+        d = _dev(x)
+        alone.append(zk.commit(d, r, ch, ht))
+        batch.append((d, r, ch, ht, zk.CommitBuffers(x.shape[1] << r, x.shape[0], ch)))
+    zk.commit_batch(batch, n_streams=4)
+    torch.cuda.synchronize()
+    for a, (_, _, _, _, o) in zip(alone, batch):
+        assert torch.equal(a.cap.view(torch.int64), o.cap.view(torch.int64))
+        assert torch.equal(a.digests.view(torch.int64), o.digests.view(torch.int64))
+        assert torch.equal(a.leaves.view(torch.int64), o.leaves.view(torch.int64))
+
+
+def test_server_results_same_alone_and_in_the_mix(zk, oracle):
+    """Every cap from the server (jobs overlapping on 4 slots under a small HBM
+    budget, so some queue) equals the same job committed alone."""
+    import torch
+
+    jobs = _mixed_jobs(oracle, 30, 11)
+    want = []
+    for x, r, ch, ht in jobs:
+        want.append(zk.commit(_dev(x), r, ch, ht).cap.cpu().numpy())
+    torch.cuda.synchronize()
+    biggest = max(x.nbytes * ((1 << r) * 2 + 1) for x, r, _, _ in jobs)
+    with zk.Server(hbm_budget_bytes=3 * biggest, slots=4) as srv:
+        tickets = [srv.submit(x, r, ch, ht) for x, r, ch, ht in jobs]
+        for t, w in zip(tickets, want):
+            cap, lat = srv.wait(t)
+            assert np.array_equal(cap, w) and lat > 0
+        # the tree stays on the device until released
+        lp, dp, cp = srv.result_ptrs(tickets[0])
+        assert lp and cp
+        st = srv.stats()
+        assert st["completed"] == len(jobs) and st["p99_s"] >= st["p50_s"] > 0
+        assert st["hbm_peak"] <= 3 * biggest
+        for t in tickets:
+            srv.release(t)
+        assert srv.stats()["hbm_in_use"] == 0
+
+
+def test_server_rejects_job_over_budget(zk, oracle):
+    x = oracle.field_elems(1, 8 << 10).reshape(8, 1 << 10)
+    with zk.Server(hbm_budget_bytes=1 << 16, slots=2) as srv:
+        t = srv.submit(x, 3, 4, 0)
+        with pytest.raises(zk.ZeknoxError):
+            srv.wait(t)
+        srv.release(t)

@@ -78,6 +78,129 @@ def transpose_rev(mat, out=None, stream=None):
     return out
 
 
+def lde_leaves(coeffs, rate_bits: int, out=None, stream=None):
+    """Forward coset LDE of (B, 2^lg_n) written as leaves: (2^(lg_n+rate_bits), B),
+    out[rev(k)][b] = LDE_b[k] (compute_batched_lde + compute_transpose_rev, fused)."""
+    import torch
+
+    assert coeffs.dtype == torch.uint64 and coeffs.is_cuda and coeffs.is_contiguous() and coeffs.dim() == 2
+    b, n = coeffs.shape
+    lg_n = n.bit_length() - 1
+    assert n == 1 << lg_n
+    if out is None:
+        out = torch.empty((n << rate_bits, b), dtype=torch.uint64, device=coeffs.device)
+    capi.check(capi.LIB.zk_lde_leaves_async(out.data_ptr(), coeffs.data_ptr(), lg_n, rate_bits, b, _stream_ptr(stream)))
+    return out
+
+
+class CommitBuffers:
+    """Device outputs of one commit: leaves (N, B), digests (2(N - 2^cap), 4), cap (2^cap, 4)."""
+
+    def __init__(self, n_leaves: int, width: int, cap_height: int, device="cuda"):
+        import torch
+
+        nd, nc = merkle_sizes(n_leaves, cap_height)
+        self.leaves = torch.empty((n_leaves, width), dtype=torch.uint64, device=device)
+        self.digests = torch.empty((max(nd, 1), 4), dtype=torch.uint64, device=device)
+        self.cap = torch.empty((nc, 4), dtype=torch.uint64, device=device)
+
+
+def commit(coeffs, rate_bits: int, cap_height: int, hash_type: int = HashPoseidon, out: CommitBuffers | None = None,
+           stream=None) -> CommitBuffers:
+    """LDE -> leaves -> Merkle forest of (B, 2^lg_n) coefficients (zk_commit_async)."""
+    b, n = coeffs.shape
+    lg_n = n.bit_length() - 1
+    if out is None:
+        out = CommitBuffers(n << rate_bits, b, cap_height, coeffs.device)
+    capi.check(capi.LIB.zk_commit_async(coeffs.data_ptr(), lg_n, rate_bits, b, cap_height, hash_type,
+                                        out.leaves.data_ptr(), out.digests.data_ptr(), out.cap.data_ptr(),
+                                        _stream_ptr(stream)))
+    return out
+
+
+def commit_batch(items, n_streams: int = 4, stream=None):
+    """items: list of (coeffs, rate_bits, cap_height, hash_type, CommitBuffers); one zk_commit_batch call."""
+    import ctypes
+
+    arr = (capi.ZkCommitJob * len(items))()
+    for i, (c, r, ch, ht, o) in enumerate(items):
+        b, n = c.shape
+        arr[i] = capi.ZkCommitJob(c.data_ptr(), n.bit_length() - 1, r, b, ch, ht, o.leaves.data_ptr(),
+                                  o.digests.data_ptr(), o.cap.data_ptr())
+    capi.check(capi.LIB.zk_commit_batch(ctypes.cast(arr, ctypes.POINTER(capi.ZkCommitJob)), len(items), n_streams,
+                                        _stream_ptr(stream)))
+
+
+class Server:
+    """Commit server (zk_server_*): continuous batching under an HBM budget."""
+
+    def __init__(self, hbm_budget_bytes: int, slots: int = 4, device: int = 0):
+        import ctypes
+
+        self._h = ctypes.c_void_p()
+        capi.check(capi.LIB.zk_server_create(device, hbm_budget_bytes, slots, ctypes.byref(self._h)))
+        self._keep = {}
+
+    def submit(self, host_coeffs, rate_bits: int, cap_height: int, hash_type: int = HashPoseidon) -> int:
+        """host_coeffs: (B, 2^lg_n) uint64 numpy array or pinned CPU tensor, kept alive until wait()."""
+        import ctypes
+
+        import numpy as np
+
+        if isinstance(host_coeffs, np.ndarray):
+            b, n = host_coeffs.shape
+            ptr = host_coeffs.ctypes.data
+        else:
+            b, n = host_coeffs.shape
+            ptr = host_coeffs.data_ptr()
+        t = ctypes.c_uint64()
+        capi.check(capi.LIB.zk_server_submit(self._h, ptr, n.bit_length() - 1, rate_bits, b, cap_height, hash_type,
+                                             ctypes.byref(t)))
+        self._keep[t.value] = (host_coeffs, cap_height)
+        return t.value
+
+    def wait(self, ticket: int):
+        """-> (cap as a (2^cap_height, 4) uint64 array, latency in seconds)."""
+        import ctypes
+
+        import numpy as np
+
+        _, ch = self._keep[ticket]
+        cap = np.zeros((1 << ch, 4), dtype=np.uint64)
+        lat = ctypes.c_double()
+        capi.check(capi.LIB.zk_server_wait(self._h, ticket, cap.ctypes.data, ctypes.byref(lat)))
+        return cap, lat.value
+
+    def result_ptrs(self, ticket: int):
+        import ctypes
+
+        l, d, c = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        capi.check(capi.LIB.zk_server_result(self._h, ticket, ctypes.byref(l), ctypes.byref(d), ctypes.byref(c)))
+        return l.value, d.value, c.value
+
+    def release(self, ticket: int):
+        capi.check(capi.LIB.zk_server_release(self._h, ticket))
+        self._keep.pop(ticket, None)
+
+    def stats(self) -> dict:
+        import ctypes
+
+        st = capi.ZkServerStats()
+        capi.check(capi.LIB.zk_server_stats(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in st._fields_}
+
+    def close(self):
+        if self._h:
+            capi.check(capi.LIB.zk_server_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def merkle_sizes(n_leaves: int, cap_height: int):
     n_caps = 1 << cap_height
     return 2 * (n_leaves - n_caps), n_caps

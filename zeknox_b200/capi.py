@@ -67,6 +67,21 @@ class TransposeConfig(ctypes.Structure):
         return cls(batches=1, are_inputs_on_device=False, are_outputs_on_device=False)
 
 
+class ZkCommitJob(ctypes.Structure):
+    """include/zeknox.h ZkCommitJob (device buffers of one commit)."""
+
+    _fields_ = [("d_coeffs", ctypes.c_void_p), ("lg_n", ctypes.c_uint32), ("rate_bits", ctypes.c_uint32),
+                ("batches", ctypes.c_uint32), ("cap_height", ctypes.c_uint32), ("hash_type", ctypes.c_uint32),
+                ("d_leaves", ctypes.c_void_p), ("d_digests", ctypes.c_void_p), ("d_cap", ctypes.c_void_p)]
+
+
+class ZkServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_uint64), ("queued", ctypes.c_uint64), ("max_queue", ctypes.c_uint64),
+                ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("max_s", ctypes.c_double),
+                ("elems", ctypes.c_double), ("elems_per_s", ctypes.c_double), ("hbm_in_use", ctypes.c_uint64),
+                ("hbm_peak", ctypes.c_uint64)]
+
+
 assert ctypes.sizeof(NTTConfig) == 24 and ctypes.sizeof(TransposeConfig) == 8
 
 
@@ -97,6 +112,16 @@ def _load() -> ctypes.CDLL:
         "zk_transpose_rev_async": (RustError, [vp, vp, u32, u32, vp]),
         "zk_merkle_async": (RustError, [vp, vp, vp, u64, u64, u64, u64, u64, u64, vp]),
         "zk_lde_noalloc": (RustError, [vp, vp, u32, u32, u32, u32, u32, vp]),
+        "zk_lde_leaves_async": (RustError, [vp, vp, u32, u32, u32, vp]),
+        "zk_commit_async": (RustError, [vp, u32, u32, u32, u32, u32, vp, vp, vp, vp]),
+        "zk_commit_batch": (RustError, [ctypes.POINTER(ZkCommitJob), u32, u32, vp]),
+        "zk_server_create": (RustError, [ctypes.c_int32, u64, u32, ctypes.POINTER(vp)]),
+        "zk_server_submit": (RustError, [vp, vp, u32, u32, u32, u32, u32, ctypes.POINTER(u64)]),
+        "zk_server_wait": (RustError, [vp, u64, vp, ctypes.POINTER(ctypes.c_double)]),
+        "zk_server_result": (RustError, [vp, u64, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)]),
+        "zk_server_release": (RustError, [vp, u64]),
+        "zk_server_stats": (RustError, [vp, ctypes.POINTER(ZkServerStats)]),
+        "zk_server_destroy": (RustError, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -105,6 +105,23 @@ void lde_device(DeviceCtx &ctx, uint64_t *d_out, const uint64_t *d_in, uint32_t 
 
 }  // namespace
 
+namespace {
+MerkleJob merkle_job(void *digests, void *cap, const void *leaves, uint64_t nd, uint64_t nc, uint64_t nl, uint64_t ls,
+                     uint64_t ch, uint64_t ht) {
+    MerkleJob j;
+    j.digests = (uint64_t *)digests;
+    j.cap = (uint64_t *)cap;
+    j.leaves = (const uint64_t *)leaves;
+    j.n_digests = nd;
+    j.n_caps = nc;
+    j.n_leaves = nl;
+    j.leaf_size = ls;
+    j.cap_height = ch;
+    j.hash_type = ht;
+    return j;
+}
+}  // namespace
+
 // ------------------------------------------------------------------ devices
 
 extern "C" RustError get_number_of_gpus(size_t *ngpus) {
@@ -307,22 +324,7 @@ extern "C" RustError compute_naive_transpose_rev(size_t device_id, void *output,
 
 // ------------------------------------------------------------------- Merkle
 
-namespace {
-MerkleJob merkle_job(void *digests, void *cap, const void *leaves, uint64_t nd, uint64_t nc, uint64_t nl, uint64_t ls,
-                     uint64_t ch, uint64_t ht) {
-    MerkleJob j;
-    j.digests = (uint64_t *)digests;
-    j.cap = (uint64_t *)cap;
-    j.leaves = (const uint64_t *)leaves;
-    j.n_digests = nd;
-    j.n_caps = nc;
-    j.n_leaves = nl;
-    j.leaf_size = ls;
-    j.cap_height = ch;
-    j.hash_type = ht;
-    return j;
-}
-}  // namespace
+
 
 // native/merkle/merkle.cu:246-280: enqueued on the legacy default stream of
 // the current device, not synchronised (gpu_id is ignored, as in zeknox).
@@ -405,6 +407,54 @@ extern "C" RustError zk_lde_async(void *d_output, const void *d_input, uint32_t 
         require(d_output && d_input, "null buffer");
         lde_device(ctx, (uint64_t *)d_output, (const uint64_t *)d_input, lg_n, rate_bits, batches, inv != 0,
                    with_coset != 0, (cudaStream_t)stream);
+    });
+}
+
+namespace {
+// Forward coset LDE written in the leaf layout: leaves[rev(k)][b] = LDE_b[k].
+void lde_leaves_device(DeviceCtx &ctx, uint64_t *d_leaves, const uint64_t *d_in, uint32_t lg_n, uint32_t rate_bits,
+                       uint64_t batches, cudaStream_t s) {
+    const uint32_t lg = lg_n + rate_bits;
+    require(lg_n >= 1 && rate_bits >= 1 && lg <= (uint32_t)kMaxLg, "invalid args");
+    NttJob j;
+    j.src = d_in;
+    j.src_stride = 1ull << lg_n;
+    j.n_valid = 1ull << lg_n;
+    j.dst = d_leaves;
+    j.batches = batches;
+    j.lg = lg;
+    j.pre_coset = &coset_table(ctx, lg, GROUP_GENERATOR, false);
+    j.to_leaves = true;
+    j.scratch_elems = ntt_scratch_elems(lg, batches);
+    Scratch scr(j.scratch_elems * sizeof(uint64_t), s);
+    j.scratch = scr.as<uint64_t>();
+    ntt_run(j, s);
+}
+}  // namespace
+
+extern "C" RustError zk_lde_leaves_async(void *d_leaves, const void *d_coeffs, uint32_t lg_n, uint32_t rate_bits,
+                                        uint32_t batches, void *stream) {
+    return guarded([&] {
+        DeviceCtx &ctx = select((size_t)current_device());
+        require(d_leaves && d_coeffs, "null buffer");
+        lde_leaves_device(ctx, (uint64_t *)d_leaves, (const uint64_t *)d_coeffs, lg_n, rate_bits, batches,
+                          (cudaStream_t)stream);
+    });
+}
+
+extern "C" RustError zk_commit_async(const void *d_coeffs, uint32_t lg_n, uint32_t rate_bits, uint32_t batches,
+                                    uint32_t cap_height, uint32_t hash_type, void *d_leaves, void *d_digests,
+                                    void *d_cap, void *stream) {
+    return guarded([&] {
+        DeviceCtx &ctx = select((size_t)current_device());
+        require(d_leaves && d_coeffs && d_cap, "null buffer");
+        const uint64_t N = 1ull << (lg_n + rate_bits);
+        const uint64_t nc = 1ull << cap_height;
+        MerkleJob m = merkle_job(d_digests, d_cap, d_leaves, 2 * (N - nc), nc, N, batches, cap_height, hash_type);
+        merkle_validate(m);  // before any work is queued
+        lde_leaves_device(ctx, (uint64_t *)d_leaves, (const uint64_t *)d_coeffs, lg_n, rate_bits, batches,
+                          (cudaStream_t)stream);
+        merkle_run(m, (cudaStream_t)stream);
     });
 }
 

@@ -44,7 +44,11 @@ struct PassArgs {
     uint32_t lg_pre;    // log2 of the number of prefixes Q = N / (L * S)
     uint32_t lg_t;      // log2 lines per group T
     uint32_t l_first;   // log2 N_1 (digit split of the prefix, 3-pass last pass)
-    uint32_t kind;      // 0 column pass, 1 last pass (rows), 2 single pass
+    uint32_t kind;      // 0 column pass, 1 last pass (rows), 2 single pass, 3 last pass to leaves
+    // leaf layout output (kinds 2 and 3): element k of polynomial b goes to
+    // dst[rev_lg(k) * leaf_stride + b] (the bit-reversing transpose, fused)
+    uint32_t to_leaves;
+    uint64_t leaf_stride;  // polynomials per leaf row (all of them, not just this chunk)
     // first pass: zero-extension and coset pre-multiply
     uint64_t n_valid;   // source elements per polynomial that are read (others are 0)
     const uint64_t *pre_lo, *pre_hi;  // coset powers (null: none)
@@ -252,6 +256,14 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
             if (a.scale != 1) v = gl_mul(v, a.scale);
             dst[o] = v;
         }
+    } else if (a.to_leaves) {
+        // leaves[rev(k)][poly0 + t]: consecutive threads write consecutive polynomials
+        for (uint32_t idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
+            const uint32_t t = idx & (T - 1), k = idx >> a.lg_t;
+            if (t >= nlines) continue;
+            const uint64_t v = sm[brev_bits(k, l) * tp + t];
+            a.dst[(uint64_t)brev_bits(k, l) * a.leaf_stride + poly0 + t] = v;
+        }
     } else {
         for (uint32_t idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
             const uint32_t k = idx & (L - 1), t = idx >> l;
@@ -263,6 +275,39 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
         }
     }
 }
+
+// Last pass of a multi-pass transform writing the leaf layout: a block takes
+// the same prefix (line krev) of 2^lg_t consecutive polynomials, so that every
+// leaf row receives 2^lg_t contiguous elements.  Element k of line krev has
+// natural index o = krev + Q k and goes to dst[rev_lg(o) * leaf_stride + b].
+__global__ void __launch_bounds__(kNttThreads) ntt_last_pass_leaves(PassArgs a) {
+    extern __shared__ uint64_t smem[];
+    const uint32_t l = a.l, L = 1u << l;
+    const uint32_t P = 1u << a.lg_t, tp = P + 1;
+    uint64_t *tw = smem;
+    uint64_t *sm = smem + L;
+    for (uint32_t j = threadIdx.x; j < L; j += blockDim.x) tw[j] = __ldg(a.line_roots + (j << (kLineLgMax - l)));
+    const uint64_t Q = 1ull << a.lg_pre;
+    const uint64_t krev = blockIdx.x % Q, pg = blockIdx.x / Q;
+    const uint64_t p0 = pg << a.lg_t;  // first polynomial of the group (within the chunk)
+    const uint32_t np = (uint32_t)min((uint64_t)P, a.batches - p0);
+    const uint64_t mask1 = (1ull << a.l_first) - 1;
+    const uint64_t kpos = ((krev & mask1) << (a.lg_pre - a.l_first)) | (krev >> a.l_first);
+    for (uint32_t idx = threadIdx.x; idx < P * L; idx += blockDim.x) {
+        const uint32_t e = idx & (L - 1), p = idx >> l;
+        sm[e * tp + p] = p < np ? a.src[(p0 + p) * a.src_poly_stride + (kpos << l) + e] : 0ull;
+    }
+    smem_dif(sm, tw, l, (int)l - 1, a.lg_t, tp);
+    const uint32_t lg = a.lg_n;
+    for (uint32_t idx = threadIdx.x; idx < P * L; idx += blockDim.x) {
+        const uint32_t p = idx & (P - 1), k = idx >> a.lg_t;
+        if (p >= np) continue;
+        const uint64_t o = krev + ((uint64_t)k << a.lg_pre);
+        const uint64_t row = __brevll(o) >> (64 - lg);
+        a.dst[row * a.leaf_stride + p0 + p] = sm[brev_bits(k, l) * tp + p];
+    }
+}
+
 
 // out[rev(k) * B + b] = in[b * N + k]: 16 rows x 64 columns per block, through
 // shared memory so both sides are coalesced (zeknox kernels.cu:94-135).
@@ -347,6 +392,19 @@ void launch_pass(const PassArgs &a, uint64_t groups, cudaStream_t s) {
     ZK_CHECK_LAUNCH();
 }
 
+void launch_leaves_pass(const PassArgs &a, uint64_t groups, cudaStream_t s) {
+    const size_t smem = pass_smem(a.l, a.lg_t);
+    static std::atomic<uint64_t> attr_set{0};
+    const int dev = current_device();
+    if (dev < 64 && !(attr_set.load() & (1ull << dev))) {
+        ZK_CUDA(cudaFuncSetAttribute(ntt_last_pass_leaves, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        attr_set.fetch_or(1ull << dev);
+    }
+    require(groups < (1ull << 31), "transform too large for one launch");
+    ntt_last_pass_leaves<<<(unsigned)groups, kNttThreads, smem, s>>>(a);
+    ZK_CHECK_LAUNCH();
+}
+
 }  // namespace
 
 // One batched transform of `batches` polynomials of 2^lg elements.
@@ -390,6 +448,11 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
         a.src_poly_stride = j.src_stride;
         a.dst_poly_stride = j.dst_stride;
         a.n_valid = j.n_valid;
+        if (j.to_leaves) {
+            a.to_leaves = 1;
+            a.leaf_stride = j.batches;
+            a.lg_t = std::min<uint32_t>(a.lg_t, 4);
+        }
         const uint64_t groups = (j.batches + (1ull << a.lg_t) - 1) >> a.lg_t;
         launch_pass(a, groups, s);
         return;
@@ -430,6 +493,20 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
                 a.scale = 1;
                 const uint64_t groups = nb << (lg - a.l - a.lg_t);
                 launch_pass(a, groups, s);
+            } else if (j.to_leaves) {
+                // 16 polynomials per block: 128-byte runs in every leaf row
+                a.kind = 3;
+                a.lg_s = 0;
+                a.lg_pre = lg - a.l;
+                a.lg_t = a.l <= 9 ? 4 : 13 - a.l;
+                a.src = scr;
+                a.src_poly_stride = N;
+                a.dst = j.dst + b0;
+                a.leaf_stride = j.batches;
+                a.pre_lo = nullptr;
+                a.n_valid = N;
+                const uint64_t groups = ((nb + (1ull << a.lg_t) - 1) >> a.lg_t) << a.lg_pre;
+                launch_leaves_pass(a, groups, s);
             } else {
                 a.kind = 1;
                 a.lg_s = 0;

@@ -28,6 +28,9 @@ struct NttJob {
     uint64_t scale = 1;
     uint64_t *scratch = nullptr;
     uint64_t scratch_elems = 0;
+    // Write the leaf layout instead: element k of polynomial b goes to
+    // dst[rev_lg(k) * batches + b] (forward transforms without post_coset/scale).
+    bool to_leaves = false;
 };
 
 void ntt_run(const NttJob &job, cudaStream_t s);

@@ -1,0 +1,497 @@
+// Batched and served commits (extensions; no zeknox counterpart).
+//
+// zk_commit_batch: many commit jobs (coset LDE -> leaves -> Merkle forest) of
+// different sizes in one call.  The caller's stream is forked onto K internal
+// streams; jobs go to streams largest-first onto the least-loaded stream (LPT),
+// so small jobs overlap with each other and with the latency-bound tops of
+// larger trees; the internal streams join back into the caller's stream.
+// Everything is stream-ordered (pool allocations included), so a batch can be
+// captured into a CUDA graph once its tables exist (run it once uncaptured).
+//
+// ZkServer: a request loop for commits that arrive over time.  A dispatcher
+// thread admits queued jobs onto free slots (one CUDA stream each) while their
+// device memory fits an HBM budget; admitted jobs run concurrently.  The tree
+// (leaves + digests + cap) of every job stays resident on the device until the
+// client releases it; the cap is also copied to the host.  Latency (submit to
+// completion of the cap copy) is recorded for p50 / p99.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/zeknox.h"
+#include "merkle.cuh"
+#include "ntt.cuh"
+#include "runtime.cuh"
+
+using namespace zk;
+
+namespace {
+
+RustError ok_err() { return RustError{0, nullptr}; }
+RustError mk_err(int code, const char *m) { return RustError{code, m ? strdup(m) : nullptr}; }
+
+template <class F>
+RustError guard(F &&f) {
+    try {
+        f();
+        return ok_err();
+    } catch (const Error &e) {
+        return mk_err(e.code, e.what());
+    } catch (const std::exception &e) {
+        return mk_err(-(int)cudaErrorUnknown, e.what());
+    }
+}
+
+struct Shape {
+    uint32_t lg_n, rate, batches, cap_h, hash;
+    uint64_t N() const { return 1ull << (lg_n + rate); }
+    uint64_t n() const { return 1ull << lg_n; }
+    uint64_t n_caps() const { return 1ull << cap_h; }
+    uint64_t n_digests() const { return 2 * (N() - n_caps()); }
+    // Work estimate: permutations (leaf sponge + nodes).
+    double work() const {
+        const uint64_t rate_words = hash == 1 ? 17 : 8;
+        return (double)N() * ((batches + rate_words - 1) / rate_words + 1);
+    }
+    uint64_t coeff_bytes() const { return n() * batches * 8; }
+    uint64_t leaf_bytes() const { return N() * batches * 8; }
+    uint64_t digest_bytes() const { return n_digests() * 32; }
+    uint64_t cap_bytes() const { return n_caps() * 32; }
+    uint64_t scratch_bytes() const { return ntt_scratch_elems(lg_n + rate, batches) * 8; }
+};
+
+void validate(const Shape &s) {
+    require(s.lg_n >= 1 && s.rate >= 1 && s.lg_n + s.rate <= 30, "invalid LDE size");
+    require(s.batches >= 1, "empty job");
+    require(s.cap_h <= s.lg_n + s.rate, "cap_height larger than the tree");
+    require(merkle_hash_supported(s.hash), "unsupported hash type");
+}
+
+// One commit on `st`: LDE in leaf layout (scratch supplied), then the forest.
+void commit_on(DeviceCtx &ctx, const Shape &sh, const uint64_t *coeffs, uint64_t *leaves, uint64_t *digests,
+               uint64_t *cap, uint64_t *scratch, cudaStream_t st) {
+    const uint32_t lg = sh.lg_n + sh.rate;
+    NttJob j;
+    j.src = coeffs;
+    j.src_stride = sh.n();
+    j.n_valid = sh.n();
+    j.dst = leaves;
+    j.batches = sh.batches;
+    j.lg = lg;
+    j.pre_coset = &coset_table(ctx, lg, GROUP_GENERATOR, false);
+    j.to_leaves = true;
+    j.scratch = scratch;
+    j.scratch_elems = ntt_scratch_elems(lg, sh.batches);
+    ntt_run(j, st);
+    MerkleJob m;
+    m.digests = digests;
+    m.cap = cap;
+    m.leaves = leaves;
+    m.n_digests = sh.n_digests();
+    m.n_caps = sh.n_caps();
+    m.n_leaves = sh.N();
+    m.leaf_size = sh.batches;
+    m.cap_height = sh.cap_h;
+    m.hash_type = sh.hash;
+    merkle_run(m, st);
+}
+
+// Per-device pool of internal streams for batches.
+struct StreamSet {
+    std::vector<cudaStream_t> s;
+    std::vector<cudaEvent_t> ev;
+};
+std::mutex g_ss_mu;
+std::unordered_map<int, std::unique_ptr<StreamSet>> g_ss;
+
+StreamSet &streams_for(int dev, uint32_t k) {
+    std::lock_guard<std::mutex> g(g_ss_mu);
+    auto &p = g_ss[dev];
+    if (!p) p = std::make_unique<StreamSet>();
+    while (p->s.size() < k) {
+        cudaStream_t st;
+        cudaEvent_t e;
+        ZK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        ZK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        p->s.push_back(st);
+        p->ev.push_back(e);
+    }
+    return *p;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------- batch
+
+extern "C" RustError zk_commit_batch(const ZkCommitJob *jobs, uint32_t n_jobs, uint32_t n_streams, void *stream) {
+    return guard([&] {
+        require(jobs != nullptr || n_jobs == 0, "null job list");
+        if (n_jobs == 0) return;
+        const int dev = current_device();
+        DeviceCtx &ctx = device_ctx(dev);
+        const uint32_t k = std::max<uint32_t>(1, std::min<uint32_t>(n_streams ? n_streams : 4, 16));
+        std::vector<Shape> sh(n_jobs);
+        for (uint32_t i = 0; i < n_jobs; i++) {
+            const ZkCommitJob &J = jobs[i];
+            sh[i] = Shape{J.lg_n, J.rate_bits, J.batches, J.cap_height, J.hash_type};
+            validate(sh[i]);
+            require(J.d_coeffs && J.d_leaves && J.d_cap && (J.d_digests || sh[i].n_digests() == 0), "null buffer");
+            // Tables first, outside any stream work (creating them synchronises).
+            coset_table(ctx, J.lg_n + J.rate_bits, GROUP_GENERATOR, false);
+            root_table(ctx, J.lg_n + J.rate_bits, false);
+        }
+        line_roots(ctx, false);
+        // LPT: largest job first onto the least-loaded stream.
+        std::vector<uint32_t> order(n_jobs);
+        for (uint32_t i = 0; i < n_jobs; i++) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return sh[a].work() > sh[b].work(); });
+        std::vector<double> load(k, 0.0);
+        std::vector<std::vector<uint32_t>> per(k);
+        std::vector<uint64_t> scratch_need(k, 0);
+        for (uint32_t i : order) {
+            const uint32_t s = (uint32_t)(std::min_element(load.begin(), load.end()) - load.begin());
+            load[s] += sh[i].work();
+            per[s].push_back(i);
+            scratch_need[s] = std::max(scratch_need[s], sh[i].scratch_bytes());
+        }
+        StreamSet &ss = streams_for(dev, k);
+        cudaStream_t caller = (cudaStream_t)stream;
+        cudaEvent_t fork;
+        ZK_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+        ZK_CUDA(cudaEventRecord(fork, caller));
+        for (uint32_t s = 0; s < k; s++) {
+            if (per[s].empty()) continue;
+            cudaStream_t st = ss.s[s];
+            ZK_CUDA(cudaStreamWaitEvent(st, fork, 0));
+            Scratch scr(scratch_need[s], st);  // one scratch per stream, reused by its jobs
+            for (uint32_t i : per[s]) {
+                const ZkCommitJob &J = jobs[i];
+                commit_on(ctx, sh[i], (const uint64_t *)J.d_coeffs, (uint64_t *)J.d_leaves, (uint64_t *)J.d_digests,
+                          (uint64_t *)J.d_cap, scr.as<uint64_t>(), st);
+            }
+            // scr is freed (stream-ordered) here, after this stream's jobs
+        }
+        for (uint32_t s = 0; s < k; s++) {
+            if (per[s].empty()) continue;
+            ZK_CUDA(cudaEventRecord(ss.ev[s], ss.s[s]));
+            ZK_CUDA(cudaStreamWaitEvent(caller, ss.ev[s], 0));
+        }
+        cudaEventDestroy(fork);
+    });
+}
+
+// ------------------------------------------------------------------ server
+
+struct ZkServer {
+    struct Job {
+        uint64_t ticket;
+        Shape sh;
+        const void *host_coeffs;
+        std::chrono::steady_clock::time_point t_submit, t_done;
+        uint64_t bytes = 0;         // device bytes held while resident
+        uint64_t run_bytes = 0;     // extra bytes held while running (coeffs + scratch)
+        uint64_t *d_coeffs = nullptr, *d_leaves = nullptr, *d_digests = nullptr, *d_cap = nullptr;
+        uint64_t *d_scratch = nullptr;
+        uint64_t *h_cap = nullptr;  // pinned copy of the cap
+        int slot = -1;
+        int state = 0;              // 0 queued, 1 running, 2 done, 3 failed
+        int err = 0;
+    };
+    int dev = 0;
+    uint64_t budget = 0, in_use = 0, peak = 0;
+    std::vector<cudaStream_t> slots;
+    std::vector<bool> slot_busy;
+    std::mutex mu;
+    std::condition_variable cv;        // dispatcher wake-up
+    std::condition_variable done_cv;   // completions
+    std::deque<uint64_t> queue;
+    std::unordered_map<uint64_t, std::unique_ptr<Job>> jobs;
+    uint64_t next_ticket = 1;
+    bool stop = false;
+    std::thread dispatcher;
+    std::vector<double> latencies;     // seconds, completed jobs
+    double elems_done = 0;
+    uint64_t max_queue = 0;
+    std::chrono::steady_clock::time_point t_first{}, t_last{};
+    bool any = false;
+    std::string fatal;
+
+    void run();
+};
+
+namespace {
+
+struct DoneCtx {
+    ZkServer *srv;
+    uint64_t ticket;
+};
+
+void CUDART_CB on_done(void *p) {
+    std::unique_ptr<DoneCtx> d((DoneCtx *)p);
+    ZkServer *srv = d->srv;
+    std::lock_guard<std::mutex> g(srv->mu);
+    auto it = srv->jobs.find(d->ticket);
+    if (it == srv->jobs.end()) return;
+    ZkServer::Job &J = *it->second;
+    J.t_done = std::chrono::steady_clock::now();
+    J.state = 2;
+    srv->slot_busy[J.slot] = false;
+    srv->in_use -= J.run_bytes;  // coeffs + scratch were freed on the stream before this point
+    srv->latencies.push_back(std::chrono::duration<double>(J.t_done - J.t_submit).count());
+    srv->elems_done += (double)J.sh.N() * J.sh.batches;
+    srv->t_last = J.t_done;
+    srv->cv.notify_all();
+    srv->done_cv.notify_all();
+}
+
+}  // namespace
+
+void ZkServer::run() {
+    ZK_CUDA(cudaSetDevice(dev));
+    DeviceCtx &ctx = device_ctx(dev);
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+        cv.wait(lk, [&] {
+            if (stop) return true;
+            if (queue.empty()) return false;
+            return std::find(slot_busy.begin(), slot_busy.end(), false) != slot_busy.end();
+        });
+        if (stop) return;
+        // A job larger than the whole budget can never run: fail it.
+        for (auto it = queue.begin(); it != queue.end();) {
+            Job &J = *jobs[*it];
+            if (J.bytes + J.run_bytes > budget) {
+                J.state = 3;
+                J.err = (int)cudaErrorMemoryAllocation;
+                done_cv.notify_all();
+                it = queue.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        // Then the first queued job, in arrival order, whose memory fits now.
+        auto pick = queue.end();
+        for (auto it = queue.begin(); it != queue.end(); ++it) {
+            const Job &J = *jobs[*it];
+            if (in_use + J.bytes + J.run_bytes <= budget) {
+                pick = it;
+                break;
+            }
+        }
+        if (pick == queue.end()) {  // nothing fits until memory is released
+            cv.wait(lk);
+            continue;
+        }
+        const uint64_t t = *pick;
+        queue.erase(pick);
+        Job &J = *jobs[t];
+        const int s = (int)(std::find(slot_busy.begin(), slot_busy.end(), false) - slot_busy.begin());
+        slot_busy[s] = true;
+        J.slot = s;
+        J.state = 1;
+        in_use += J.bytes + J.run_bytes;
+        peak = std::max(peak, in_use);
+        lk.unlock();
+        try {
+            cudaStream_t st = slots[s];
+            const Shape &sh = J.sh;
+            ZK_CUDA(cudaMallocAsync((void **)&J.d_coeffs, sh.coeff_bytes(), st));
+            ZK_CUDA(cudaMallocAsync((void **)&J.d_leaves, sh.leaf_bytes(), st));
+            if (sh.n_digests()) ZK_CUDA(cudaMallocAsync((void **)&J.d_digests, sh.digest_bytes(), st));
+            ZK_CUDA(cudaMallocAsync((void **)&J.d_cap, sh.cap_bytes(), st));
+            if (sh.scratch_bytes()) ZK_CUDA(cudaMallocAsync((void **)&J.d_scratch, sh.scratch_bytes(), st));
+            ZK_CUDA(cudaMemcpyAsync(J.d_coeffs, J.host_coeffs, sh.coeff_bytes(), cudaMemcpyHostToDevice, st));
+            commit_on(ctx, sh, J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch, st);
+            ZK_CUDA(cudaMemcpyAsync(J.h_cap, J.d_cap, sh.cap_bytes(), cudaMemcpyDeviceToHost, st));
+            ZK_CUDA(cudaFreeAsync(J.d_coeffs, st));
+            J.d_coeffs = nullptr;
+            if (J.d_scratch) ZK_CUDA(cudaFreeAsync(J.d_scratch, st));
+            J.d_scratch = nullptr;
+            ZK_CUDA(cudaLaunchHostFunc(st, on_done, new DoneCtx{this, t}));
+        } catch (const std::exception &e) {
+            lk.lock();
+            J.state = 3;
+            J.err = -1;
+            slot_busy[s] = false;
+            in_use -= J.bytes + J.run_bytes;
+            fatal = e.what();
+            done_cv.notify_all();
+            continue;
+        }
+        lk.lock();
+    }
+}
+
+extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes, uint32_t n_slots, ZkServer **out) {
+    return guard([&] {
+        require(out != nullptr && n_slots >= 1 && n_slots <= 64 && hbm_budget_bytes > 0, "invalid server arguments");
+        ZK_CUDA(cudaSetDevice(device));
+        device_ctx(device);
+        auto srv = std::make_unique<ZkServer>();
+        srv->dev = device;
+        srv->budget = hbm_budget_bytes;
+        for (uint32_t i = 0; i < n_slots; i++) {
+            cudaStream_t st;
+            ZK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            srv->slots.push_back(st);
+            srv->slot_busy.push_back(false);
+        }
+        ZkServer *p = srv.get();
+        srv->dispatcher = std::thread([p] {
+            try {
+                p->run();
+            } catch (const std::exception &e) {
+                std::lock_guard<std::mutex> g(p->mu);
+                p->fatal = e.what();
+                p->done_cv.notify_all();
+            }
+        });
+        *out = srv.release();
+    });
+}
+
+extern "C" RustError zk_server_submit(ZkServer *srv, const void *host_coeffs, uint32_t lg_n, uint32_t rate_bits,
+                                     uint32_t batches, uint32_t cap_height, uint32_t hash_type, uint64_t *ticket) {
+    return guard([&] {
+        require(srv && host_coeffs && ticket, "null argument");
+        Shape sh{lg_n, rate_bits, batches, cap_height, hash_type};
+        validate(sh);
+        {
+            // Tables are created on the caller's thread, before the job can run.
+            ZK_CUDA(cudaSetDevice(srv->dev));
+            DeviceCtx &ctx = device_ctx(srv->dev);
+            coset_table(ctx, lg_n + rate_bits, GROUP_GENERATOR, false);
+            root_table(ctx, lg_n + rate_bits, false);
+            line_roots(ctx, false);
+        }
+        auto J = std::make_unique<ZkServer::Job>();
+        J->sh = sh;
+        J->host_coeffs = host_coeffs;
+        J->bytes = sh.leaf_bytes() + sh.digest_bytes() + sh.cap_bytes();
+        J->run_bytes = sh.coeff_bytes() + sh.scratch_bytes();
+        ZK_CUDA(cudaMallocHost((void **)&J->h_cap, sh.cap_bytes()));
+        std::lock_guard<std::mutex> g(srv->mu);
+        require(srv->fatal.empty(), "server failed: " + srv->fatal);
+        J->ticket = srv->next_ticket++;
+        J->t_submit = std::chrono::steady_clock::now();
+        if (!srv->any) {
+            srv->t_first = J->t_submit;
+            srv->any = true;
+        }
+        *ticket = J->ticket;
+        srv->queue.push_back(J->ticket);
+        srv->max_queue = std::max<uint64_t>(srv->max_queue, srv->queue.size());
+        srv->jobs[J->ticket] = std::move(J);
+        srv->cv.notify_all();
+    });
+}
+
+extern "C" RustError zk_server_wait(ZkServer *srv, uint64_t ticket, uint64_t *host_cap, double *latency_s) {
+    return guard([&] {
+        require(srv != nullptr, "null server");
+        std::unique_lock<std::mutex> lk(srv->mu);
+        auto it = srv->jobs.find(ticket);
+        require(it != srv->jobs.end(), "unknown ticket");
+        ZkServer::Job *J = it->second.get();
+        srv->done_cv.wait(lk, [&] { return J->state >= 2 || !srv->fatal.empty(); });
+        require(J->state == 2, J->err == (int)cudaErrorMemoryAllocation ? "job larger than the HBM budget"
+                                                                          : "job failed: " + srv->fatal);
+        if (host_cap) memcpy(host_cap, J->h_cap, J->sh.cap_bytes());
+        if (latency_s) *latency_s = std::chrono::duration<double>(J->t_done - J->t_submit).count();
+    });
+}
+
+extern "C" RustError zk_server_result(ZkServer *srv, uint64_t ticket, void **d_leaves, void **d_digests,
+                                     void **d_cap) {
+    return guard([&] {
+        require(srv != nullptr, "null server");
+        std::lock_guard<std::mutex> g(srv->mu);
+        auto it = srv->jobs.find(ticket);
+        require(it != srv->jobs.end() && it->second->state == 2, "ticket not completed");
+        if (d_leaves) *d_leaves = it->second->d_leaves;
+        if (d_digests) *d_digests = it->second->d_digests;
+        if (d_cap) *d_cap = it->second->d_cap;
+    });
+}
+
+extern "C" RustError zk_server_release(ZkServer *srv, uint64_t ticket) {
+    return guard([&] {
+        require(srv != nullptr, "null server");
+        std::unique_ptr<ZkServer::Job> J;
+        {
+            std::lock_guard<std::mutex> g(srv->mu);
+            auto it = srv->jobs.find(ticket);
+            require(it != srv->jobs.end(), "unknown ticket");
+            require(it->second->state >= 2, "ticket still running");
+            J = std::move(it->second);
+            srv->jobs.erase(it);
+        }
+        ZK_CUDA(cudaSetDevice(srv->dev));
+        if (J->state == 2) {
+            cudaStream_t st = srv->slots[J->slot];
+            if (J->d_leaves) ZK_CUDA(cudaFreeAsync(J->d_leaves, st));
+            if (J->d_digests) ZK_CUDA(cudaFreeAsync(J->d_digests, st));
+            if (J->d_cap) ZK_CUDA(cudaFreeAsync(J->d_cap, st));
+            std::lock_guard<std::mutex> g(srv->mu);
+            srv->in_use -= J->bytes;
+            srv->cv.notify_all();
+        }
+        cudaFreeHost(J->h_cap);
+    });
+}
+
+extern "C" RustError zk_server_stats(ZkServer *srv, ZkServerStats *out) {
+    return guard([&] {
+        require(srv && out, "null argument");
+        std::lock_guard<std::mutex> g(srv->mu);
+        std::vector<double> l = srv->latencies;
+        std::sort(l.begin(), l.end());
+        auto pct = [&](double q) { return l.empty() ? 0.0 : l[std::min<size_t>(l.size() - 1, (size_t)(q * l.size()))]; };
+        memset(out, 0, sizeof(*out));
+        out->completed = l.size();
+        out->queued = srv->queue.size();
+        out->max_queue = srv->max_queue;
+        out->p50_s = pct(0.50);
+        out->p99_s = pct(0.99);
+        out->max_s = l.empty() ? 0 : l.back();
+        out->elems = srv->elems_done;
+        const double span = srv->any ? std::chrono::duration<double>(srv->t_last - srv->t_first).count() : 0.0;
+        out->elems_per_s = span > 0 ? srv->elems_done / span : 0.0;
+        out->hbm_in_use = srv->in_use;
+        out->hbm_peak = srv->peak;
+    });
+}
+
+extern "C" RustError zk_server_destroy(ZkServer *srv) {
+    if (!srv) return ok_err();
+    {
+        std::lock_guard<std::mutex> g(srv->mu);
+        srv->stop = true;
+        srv->cv.notify_all();
+    }
+    if (srv->dispatcher.joinable()) srv->dispatcher.join();
+    RustError r = guard([&] {
+        ZK_CUDA(cudaSetDevice(srv->dev));
+        for (cudaStream_t st : srv->slots) ZK_CUDA(cudaStreamSynchronize(st));
+        for (auto &kv : srv->jobs) {
+            auto &J = *kv.second;
+            for (uint64_t *p : {J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch})
+                if (p) cudaFree(p);
+            if (J.h_cap) cudaFreeHost(J.h_cap);
+        }
+        for (cudaStream_t st : srv->slots) cudaStreamDestroy(st);
+    });
+    delete srv;
+    return r;
+}
