@@ -205,7 +205,16 @@ def main() -> None:
     ap.add_argument("--rate-bits", type=int, default=3)
     ap.add_argument("--cap-height", type=int, default=4)
     ap.add_argument("--hash", default="poseidon", choices=sorted(HASH_NAMES))
+    ap.add_argument("--workload", default="commit", choices=["commit", "merkle", "sweep", "batched", "served"],
+                    help="commit (default, the bench line); the others print their own JSON summary")
+    ap.add_argument("--jobs", type=int, default=0)
+    ap.add_argument("--streams", type=int, default=4)
+    ap.add_argument("--budget-gb", type=int, default=120)
+    ap.add_argument("--rates", type=float, nargs="*", default=[0.5, 1.0, 1.25])
     args = ap.parse_args()
+    if args.workload != "commit" and args.impl == "ours":
+        {"merkle": run_merkle_only, "sweep": run_sweep, "batched": run_batched, "served": run_served}[args.workload](args)
+        return
     set_workload(args.polys, args.lg_n, args.rate_bits, args.cap_height, args.hash)
     if args.impl == "reference":
         run_reference(args)
@@ -238,46 +247,59 @@ def main() -> None:
     cap = torch.empty((nc, 4), dtype=torch.uint64, device=dev)
     stream = torch.cuda.current_stream()
 
-    ev = {}
-
-    def step(i: int, timed: bool = False):
-        if timed:
-            ev.setdefault("e", []).append([torch.cuda.Event(enable_timing=True) for _ in range(4)])
-            e = ev["e"][-1]
-            e[0].record(stream)
-        zk.lde(coeffs[i % N_ROT], RATE, out=lde_out)
-        if timed:
-            e[1].record(stream)
-        zk.transpose_rev(lde_out, out=leaves)
-        if timed:
-            e[2].record(stream)
-        zk.merkle_tree(leaves, CAP_H, HASH, digests, cap)
-        if timed:
-            e[3].record(stream)
-
     def barrier():
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
             torch.cuda.synchronize()
 
-    for w in range(args.warmup):
-        step(w)
-    barrier()
-    launches0 = zk.capi.LIB.zk_kernel_launches()
-    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        t_start.record(stream)
+    def timed_loop(step, n_phases):
+        """W warm-up steps, then K timed steps with an event after each phase."""
+        for w in range(args.warmup):
+            step(w, None)
+        barrier()
+        evs = []
+        t0e, t1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0e.record(stream)
         for k in range(args.steps):
-            step(k, timed=True)
-        t_end.record(stream)
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(n_phases + 1)]
+            e[0].record(stream)
+            step(k, e)
+            evs.append(e)
+        t1e.record(stream)
         torch.cuda.synchronize()
-    launches = zk.capi.LIB.zk_kernel_launches() - launches0
-    ms = t_start.elapsed_time(t_end)
-    phase = np.array([[e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), e[2].elapsed_time(e[3])] for e in ev["e"]])
-    t_lde, t_tr, t_mk = (float(x) for x in phase.mean(axis=0))
+        phases = np.array([[e[i].elapsed_time(e[i + 1]) for i in range(n_phases)] for e in evs]).mean(axis=0)
+        return t0e.elapsed_time(t1e), [float(x) for x in phases]
+
+    # ---- the timed region: fused commit (LDE written as leaves, then the forest) ----
+    def fused_step(i, e):
+        zk.lde_leaves(coeffs[i % N_ROT], RATE, out=leaves)
+        if e:
+            e[1].record(stream)
+        zk.merkle_tree(leaves, CAP_H, HASH, digests, cap)
+        if e:
+            e[2].record(stream)
+
+    launches0 = zk.capi.LIB.zk_kernel_launches()
+    with ClockSampler(local) as clk:
+        ms, (t_lde, t_mk) = timed_loop(fused_step, 2)
+    launches = (zk.capi.LIB.zk_kernel_launches() - launches0) * args.steps // (args.steps + args.warmup)
     cap_dev = cap.cpu().numpy().copy()
     gpu_cap_input = (args.steps - 1) % N_ROT
+
+    # ---- the plain drop-in device path: LDE matrix, transpose, forest ----
+    def plain_step(i, e):
+        zk.lde(coeffs[i % N_ROT], RATE, out=lde_out)
+        if e:
+            e[1].record(stream)
+        zk.transpose_rev(lde_out, out=leaves)
+        if e:
+            e[2].record(stream)
+        zk.merkle_tree(leaves, CAP_H, HASH, digests, cap)
+        if e:
+            e[3].record(stream)
+
+    ms_plain, (p_lde, p_tr, p_mk) = timed_loop(plain_step, 3)
 
     # ---- end to end through the C ABI with host buffers ----
     pinned = [torch.from_numpy(c).pin_memory() for c in host_coeffs]
@@ -310,10 +332,10 @@ def main() -> None:
     e2e_input = (args.steps - 1) % N_ROT
 
     # ---- max over ranks ----
-    ms_t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
+    ms_t = torch.tensor([ms, e2e_s, ms_plain], dtype=torch.float64, device=dev)
     if dist is not None:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max, e2e_max = float(ms_t[0]), float(ms_t[1])
+    ms_max, e2e_max, ms_plain = float(ms_t[0]), float(ms_t[1]), float(ms_t[2])
 
     if rank == 0:
         value = world * B * N * args.steps / (ms_max * 1e-3)
@@ -334,12 +356,12 @@ def main() -> None:
                            "has no integer figure)",
             "ms_per_launch": t_mk,
         }
-        hbm_bytes = LDE_BYTES + TRANSPOSE_BYTES
+        hbm_bytes = LDE_BYTES
         roof_hbm = {
-            "kernel": "LDE (2 shared-memory passes) + transpose_rev", "bound": "hbm", "unit": "GB/s",
-            "achieved": hbm_bytes / ((t_lde + t_tr) * 1e-3) / 1e9, "peak": hbm_peak,
-            "frac": (hbm_bytes / ((t_lde + t_tr) * 1e-3) / 1e9) / hbm_peak if hbm_peak else None,
-            "traffic": None, "algorithmic_bytes": hbm_bytes, "ms_lde": t_lde, "ms_transpose": t_tr,
+            "kernel": "LDE written as leaves (2 shared-memory NTT passes)", "bound": "hbm", "unit": "GB/s",
+            "achieved": hbm_bytes / (t_lde * 1e-3) / 1e9, "peak": hbm_peak,
+            "frac": (hbm_bytes / (t_lde * 1e-3) / 1e9) / hbm_peak if hbm_peak else None,
+            "traffic": None, "algorithmic_bytes": hbm_bytes, "ms_per_launch": t_lde,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm_peak else None,
         }
         out = {
@@ -356,7 +378,11 @@ def main() -> None:
                     "path": "compute_batched_lde (pinned host in) -> compute_transpose_rev -> "
                             "fill_digests_buf_linear_gpu_with_gpu_ptr -> D2H digests+cap"},
             "gpu_launches": int(launches),
-            "phases_ms": {"lde": t_lde, "transpose": t_tr, "merkle": t_mk},
+            "phases_ms": {"lde_to_leaves": t_lde, "merkle": t_mk},
+            "plain_device_path": {"value": world * B * N * args.steps / (ms_plain * 1e-3), "unit": "elems/s",
+                                  "ms_per_step": ms_plain / args.steps,
+                                  "phases_ms": {"lde": p_lde, "transpose": p_tr, "merkle": p_mk},
+                                  "path": "zk_lde_async -> zk_transpose_rev_async -> zk_merkle_async"},
             "roofline": roof,
             "roofline_hbm": roof_hbm,
             "clocks": clk.summary(),
@@ -380,6 +406,257 @@ def main() -> None:
         dist.barrier()
         dist.destroy_process_group()
 
+
+# ------------------------------------------------------------------ other workloads
+def _device_pool(torch, elems: int, seed: int):
+    """Device buffer of canonical field elements (values < 2^62), shared by jobs as input."""
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    return torch.randint(0, 2**62, (elems,), generator=g, device="cuda", dtype=torch.int64).view(torch.uint64)
+
+
+def _ev_ms(torch, fn, reps=1):
+    s = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for _ in range(reps):
+        fn()
+    b.record(s)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def run_merkle_only(args):
+    """Plain Poseidon Merkle tree, 8192 leaves x 135, cap height 4 (the reference's own CPU-runnable case)."""
+    import torch
+
+    import zeknox_b200 as zk
+
+    nl, w, ch = 8192, 135, 4
+    host = field_elems(0x5EED0001, nl * w)
+    leaves = torch.from_numpy(host).cuda().view(nl, w)
+    d, c = zk.merkle_tree(leaves, ch, 0)
+    for _ in range(args.warmup):
+        zk.merkle_tree(leaves, ch, 0, d, c)
+    ms = _ev_ms(torch, lambda: zk.merkle_tree(leaves, ch, 0, d, c), args.steps)
+    perms = nl * 17 + nl
+    out = {"workload": "merkle 8192x135 poseidon cap_height 4", "ms": ms, "perm_per_s": perms / (ms * 1e-3),
+           "leaf_elems_per_s": nl * w / (ms * 1e-3)}
+    from oracle import oracle as O
+
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    t0 = time.perf_counter()
+    _, cap_ref = O.ref_merkle_fill(host, w, ch, 0) if O.ref_available() else O.merkle_fill(host, w, ch, 0)
+    out["cpu_reference_ms"] = (time.perf_counter() - t0) * 1e3
+    out["cap_equals_cpu_reference"] = bool(np.array_equal(cap_ref.reshape(-1, 4), c.cpu().numpy()))
+    print(json.dumps(out), flush=True)
+
+
+def run_sweep(args):
+    """Hash sweep: 2^20 leaves x 135, cap height 4, Poseidon / Poseidon2 / Keccak."""
+    import torch
+
+    import zeknox_b200 as zk
+
+    nl, w, ch = 1 << 20, 135, 4
+    leaves = _device_pool(torch, nl * w, 0x5EED0004).view(nl, w)
+    peak = int32_peak()
+    res = {"workload": "merkle sweep 2^20 x 135, cap_height 4", "int32_peak_gops": peak / 1e9 if peak else None}
+    for name, ht in (("poseidon", 0), ("poseidon2", 3), ("keccak", 1)):
+        d, c = zk.merkle_tree(leaves, ch, ht)
+        for _ in range(args.warmup):
+            zk.merkle_tree(leaves, ch, ht, d, c)
+        ms = _ev_ms(torch, lambda: zk.merkle_tree(leaves, ch, ht, d, c), max(3, args.steps // 4))
+        rate_words = 17 if ht == 1 else 8
+        perms = nl * ((w + rate_words - 1) // rate_words) + nl
+        ops = perms * OPS_PER_PERM[ht]
+        res[name] = {"ms": ms, "perm_per_s": perms / (ms * 1e-3), "leaf_elems_per_s": nl * w / (ms * 1e-3),
+                     "int32_frac": ops / (ms * 1e-3) / peak if peak else None}
+    # zeknox's CPU path on a 2^14-leaf sample of the same shape
+    from oracle import oracle as O
+
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    sample = leaves[: 1 << 14].cpu().numpy().reshape(-1)
+    for name, ht in (("poseidon", 0), ("poseidon2", 3), ("keccak", 1)):
+        t0 = time.perf_counter()
+        (O.ref_merkle_fill if O.ref_available() else O.merkle_fill)(sample, w, ch, ht)
+        res[name]["cpu_reference_leaf_elems_per_s"] = (1 << 14) * w / (time.perf_counter() - t0)
+    print(json.dumps(res), flush=True)
+
+
+def _jobs(seed, count, lg_lo, lg_hi, b_lo, b_hi, rates):
+    rng = np.random.default_rng(seed)
+    return [(int(rng.integers(lg_lo, lg_hi + 1)), int(rng.integers(b_lo, b_hi + 1)), int(rng.choice(rates)))
+            for _ in range(count)]
+
+
+def _plain_job(zk, torch, coeffs, lg_n, rate, b, ch, bufs):
+    """One job through zeknox's drop-in C ABI: LDE matrix, transpose, forest, sync."""
+    N = 1 << (lg_n + rate)
+    lde_out, leaves, digests, cap = bufs
+    cfg = zk.NTTConfig.default()
+    cfg.batches, cfg.extension_rate_bits, cfg.with_coset = b, rate, True
+    cfg.are_inputs_on_device = cfg.are_outputs_on_device = True
+    zk.lde_batch(0, lde_out.data_ptr(), coeffs.data_ptr(), lg_n, cfg)
+    t = zk.TransposeConfig.default()
+    t.batches, t.are_inputs_on_device, t.are_outputs_on_device = b, True, True
+    zk.transpose_rev_batch(0, leaves.data_ptr(), lde_out.data_ptr(), lg_n + rate, t)
+    zk.fill_digests_buf_linear_gpu_with_gpu_ptr(digests.data_ptr(), cap.data_ptr(), leaves.data_ptr(),
+                                                2 * (N - (1 << ch)), 1 << ch, N, b, ch, 0, 0)
+    torch.cuda.synchronize()
+
+
+def run_batched(args):
+    """256 jobs: lg_n in 12..20, polys 4..200, rate 1..3, cap height 4, Poseidon; one zk_commit_batch
+    call per memory wave vs the plain per-job drop-in path."""
+    import torch
+
+    import zeknox_b200 as zk
+
+    jobs = _jobs(0x5EED0003, args.jobs or 256, 12, 20, 4, 200, [1, 2, 3])
+    ch = 4
+    pool = _device_pool(torch, max(b << lg for lg, b, _ in jobs), 0x5EED0003)
+    elems = sum(b << (lg + r) for lg, b, r in jobs)
+    mx = max(b << (lg + r) for lg, b, r in jobs)
+    mx_n = max(1 << (lg + r) for lg, b, r in jobs)
+    bufs = (torch.empty(mx, dtype=torch.uint64, device="cuda"), torch.empty(mx, dtype=torch.uint64, device="cuda"),
+            torch.empty(8 * mx_n, dtype=torch.uint64, device="cuda"), torch.empty(64, dtype=torch.uint64, device="cuda"))
+    zk.init_coset(0, 23, 7)
+    for lg, b, r in jobs[:4]:  # warm-up
+        _plain_job(zk, torch, pool[: b << lg], lg, r, b, ch, bufs)
+    t0 = time.perf_counter()
+    for lg, b, r in jobs:
+        _plain_job(zk, torch, pool[: b << lg], lg, r, b, ch, bufs)
+    t_plain = time.perf_counter() - t0
+    del bufs
+    torch.cuda.empty_cache()
+    # batched: waves of jobs whose outputs fit a budget
+    budget = args.budget_gb << 30
+    waves, cur, used = [], [], 0
+    for j in sorted(jobs, key=lambda j: -(j[1] << (j[0] + j[2]))):
+        need = (j[1] << (j[0] + j[2])) * 8 + (2 << (j[0] + j[2])) * 32
+        if cur and used + need > budget:
+            waves.append(cur)
+            cur, used = [], 0
+        cur.append(j)
+        used += need
+    waves.append(cur)
+    outs = []
+    t0 = time.perf_counter()
+    for wave in waves:
+        items = []
+        for lg, b, r in wave:
+            items.append((pool[: b << lg].view(b, 1 << lg), r, ch, 0, zk.CommitBuffers(1 << (lg + r), b, ch)))
+        zk.commit_batch(items, n_streams=args.streams)
+        torch.cuda.synchronize()
+        outs.append(items[0][4].cap.cpu())
+        del items
+    t_batch = time.perf_counter() - t0
+    print(json.dumps({"workload": f"batched commit: {len(jobs)} jobs lg_n 12..20, polys 4..200, rate 1..3, "
+                                  "cap_height 4, poseidon",
+                      "elems": elems, "plain_per_job_elems_per_s": elems / t_plain,
+                      "batched_elems_per_s": elems / t_batch, "batched_over_plain": t_plain / t_batch,
+                      "plain_s": t_plain, "batched_s": t_batch, "waves": len(waves), "streams": args.streams,
+                      "budget_gb": args.budget_gb}), flush=True)
+
+
+def run_served(args):
+    """Served stream: jobs lg_n 12..22, polys 8..300, rate 3, cap height 4, Poseidon, Poisson arrivals at
+    fractions of the plain path's capacity; the server (HBM budget, concurrent slots) vs a FIFO queue
+    served by the plain per-job drop-in path."""
+    import torch
+
+    import zeknox_b200 as zk
+
+    n_jobs = args.jobs or 40
+    ch, r = 4, 3
+    stream = _jobs(0x5EED0005, 10000, 12, 22, 8, 300, [3])  # the seeded 10,000-job stream
+    # The drop-in path holds the LDE matrix and the leaves (2 x 8 B per point): keep the first jobs for
+    # which that fits next to the input in HBM, so both paths run the same jobs.
+    jobs = [j for j in stream if (j[1] << (j[0] + r)) * 16 + (j[1] << j[0]) * 8 <= 140 << 30][:n_jobs]
+    mx_in = max(b << lg for lg, b, _ in jobs)
+    mx = max(b << (lg + r) for lg, b, _ in jobs)
+    mx_n = max(1 << (lg + r) for lg, _, _ in jobs)
+    host = torch.empty(mx_in, dtype=torch.uint64).pin_memory()
+    host.view(torch.int64).copy_(_device_pool(torch, mx_in, 0x5EED0005).view(torch.int64).cpu())
+    zk.init_coset(0, 25, 7)
+    dev_in = torch.empty(mx_in, dtype=torch.uint64, device="cuda")
+    bufs = (torch.empty(mx, dtype=torch.uint64, device="cuda"), torch.empty(mx, dtype=torch.uint64, device="cuda"),
+            torch.empty(8 * mx_n, dtype=torch.uint64, device="cuda"), torch.empty(64, dtype=torch.uint64, device="cuda"))
+
+    def plain(lg, b):  # host coefficients in, as a served request would arrive
+        dev_in[: b << lg].copy_(host[: b << lg])
+        _plain_job(zk, torch, dev_in[: b << lg], lg, r, b, ch, bufs)
+
+    plain(*jobs[0][:2])
+    service = []
+    for lg, b, _ in jobs:
+        t0 = time.perf_counter()
+        plain(lg, b)
+        service.append(time.perf_counter() - t0)
+    cap_jobs_per_s = n_jobs / sum(service)
+    elems = sum(b << (lg + r) for lg, b, _ in jobs)
+    res = {"workload": f"served: {n_jobs} jobs of the seeded 10,000-job stream (lg_n 12..22, polys 8..300, "
+                       "rate 3, cap_height 4, poseidon; jobs whose drop-in path fits in HBM)",
+           "plain_capacity_jobs_per_s": cap_jobs_per_s, "plain_capacity_elems_per_s": elems / sum(service),
+           "slots": args.streams, "budget_gb": args.budget_gb, "rates": {}}
+    rng = np.random.default_rng(0x5EED0055)
+    arrivals = {f: np.cumsum(rng.exponential(1.0 / (f * cap_jobs_per_s), n_jobs)) for f in args.rates}
+    # plain path first: one FIFO queue, one job per call, in real time
+    plain_res = {}
+    for f in args.rates:
+        lat = []
+        t0 = time.perf_counter()
+        for a, (lg, b, _) in zip(arrivals[f], jobs):
+            now = time.perf_counter() - t0
+            if now < a:
+                time.sleep(a - now)
+            plain(lg, b)
+            lat.append(time.perf_counter() - t0 - a)
+        plain_res[f] = (lat, time.perf_counter() - t0)
+    # free the plain path's buffers: the server owns the HBM budget from here
+    del bufs, dev_in
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    import queue
+    import threading
+
+    for f in args.rates:
+        with zk.Server(hbm_budget_bytes=args.budget_gb << 30, slots=args.streams) as srv:
+            q: queue.Queue = queue.Queue()
+            lat_s = []
+
+            def client():
+                while True:
+                    t = q.get()
+                    if t is None:
+                        return
+                    _, l = srv.wait(t)
+                    lat_s.append(l)
+                    srv.release(t)
+
+            th = threading.Thread(target=client)
+            th.start()
+            t0 = time.perf_counter()
+            for a, (lg, b, _) in zip(arrivals[f], jobs):
+                now = time.perf_counter() - t0
+                if now < a:
+                    time.sleep(a - now)
+                q.put(srv.submit(host[: b << lg].view(b, 1 << lg), r, ch, 0))
+            q.put(None)
+            th.join()
+            span_srv = time.perf_counter() - t0
+            st = srv.stats()
+        lat, span_plain = plain_res[f]
+        res["rates"][str(f)] = {
+            "arrival_jobs_per_s": f * cap_jobs_per_s,
+            "plain": {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                      "elems_per_s": elems / span_plain},
+            "served": {"p50_s": float(np.percentile(lat_s, 50)), "p99_s": float(np.percentile(lat_s, 99)),
+                       "elems_per_s": elems / span_srv, "max_queue": st["max_queue"],
+                       "hbm_peak_gb": st["hbm_peak"] / 2**30},
+        }
+        print(json.dumps({"rate": f, **res["rates"][str(f)]}), flush=True)
+    print(json.dumps(res), flush=True)
 
 if __name__ == "__main__":
     main()

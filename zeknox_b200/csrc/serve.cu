@@ -9,11 +9,16 @@
 // captured into a CUDA graph once its tables exist (run it once uncaptured).
 //
 // ZkServer: a request loop for commits that arrive over time.  A dispatcher
-// thread admits queued jobs onto free slots (one CUDA stream each) while their
-// device memory fits an HBM budget; admitted jobs run concurrently.  The tree
-// (leaves + digests + cap) of every job stays resident on the device until the
-// client releases it; the cap is also copied to the host.  Latency (submit to
-// completion of the cap copy) is recorded for p50 / p99.
+// thread admits queued jobs onto free slots while their device memory fits an
+// HBM budget; admitted jobs run concurrently.  Admission is shortest-job-first
+// with aging (a job's estimated GPU time minus half the time it has waited),
+// at most one large job runs at a time (two large trees sharing the GPU only
+// delay each other), and each job's stream gets a CUDA priority by size, so
+// small commits are scheduled onto SMs ahead of the blocks of a large one
+// that is already running.  The tree (leaves + digests + cap) of every job
+// stays resident on the device until the client releases it; the cap is also
+// copied to the host.  Latency (submit to completion of the cap copy) is
+// recorded for p50 / p99.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -205,13 +210,17 @@ struct ZkServer {
         uint64_t *d_scratch = nullptr;
         uint64_t *h_cap = nullptr;  // pinned copy of the cap
         int slot = -1;
+        double est_s = 0;           // estimated GPU time
+        cudaStream_t stream = nullptr;  // the stream the job ran on
+        bool big = false;
         int state = 0;              // 0 queued, 1 running, 2 done, 3 failed
         int err = 0;
     };
     int dev = 0;
     uint64_t budget = 0, in_use = 0, peak = 0;
-    std::vector<cudaStream_t> slots;
+    std::vector<std::vector<cudaStream_t>> slots;  // [slot][priority level]: level 0 highest
     std::vector<bool> slot_busy;
+    int running_big = 0;
     std::mutex mu;
     std::condition_variable cv;        // dispatcher wake-up
     std::condition_variable done_cv;   // completions
@@ -247,6 +256,7 @@ void CUDART_CB on_done(void *p) {
     J.t_done = std::chrono::steady_clock::now();
     J.state = 2;
     srv->slot_busy[J.slot] = false;
+    if (J.big) srv->running_big--;
     srv->in_use -= J.run_bytes;  // coeffs + scratch were freed on the stream before this point
     srv->latencies.push_back(std::chrono::duration<double>(J.t_done - J.t_submit).count());
     srv->elems_done += (double)J.sh.N() * J.sh.batches;
@@ -280,15 +290,25 @@ void ZkServer::run() {
                 ++it;
             }
         }
-        // Then the first queued job, in arrival order, whose memory fits now.
-        auto pick = queue.end();
+        // Then the queued job that fits now with the smallest estimated GPU
+        // time minus half its waiting time (shortest-job-first with aging); a
+        // large job waits while another large job runs, unless nothing else can go.
+        auto pick = queue.end(), pick_big = queue.end();
+        double best = 1e300, best_big = 1e300;
+        const auto now = std::chrono::steady_clock::now();
         for (auto it = queue.begin(); it != queue.end(); ++it) {
             const Job &J = *jobs[*it];
-            if (in_use + J.bytes + J.run_bytes <= budget) {
-                pick = it;
-                break;
+            if (in_use + J.bytes + J.run_bytes > budget) continue;
+            const double key = J.est_s - 0.5 * std::chrono::duration<double>(now - J.t_submit).count();
+            if (J.big && running_big > 0) {
+                if (key < best_big) best_big = key, pick_big = it;
+                continue;
             }
+            if (key < best) best = key, pick = it;
         }
+        if (pick == queue.end() && pick_big != queue.end() &&
+            std::find(slot_busy.begin(), slot_busy.end(), true) == slot_busy.end())
+            pick = pick_big;  // the GPU is idle: run it anyway
         if (pick == queue.end()) {  // nothing fits until memory is released
             cv.wait(lk);
             continue;
@@ -300,11 +320,16 @@ void ZkServer::run() {
         slot_busy[s] = true;
         J.slot = s;
         J.state = 1;
+        if (J.big) running_big++;
         in_use += J.bytes + J.run_bytes;
         peak = std::max(peak, in_use);
         lk.unlock();
         try {
-            cudaStream_t st = slots[s];
+            // priority by size: < 20 ms of estimated GPU time highest, < 200 ms next, larger lowest
+            const int nlev = (int)slots[s].size();
+            const int lev = J.est_s < 0.02 ? 0 : J.est_s < 0.2 ? std::min(1, nlev - 1) : nlev - 1;
+            cudaStream_t st = slots[s][lev];
+            J.stream = st;
             const Shape &sh = J.sh;
             ZK_CUDA(cudaMallocAsync((void **)&J.d_coeffs, sh.coeff_bytes(), st));
             ZK_CUDA(cudaMallocAsync((void **)&J.d_leaves, sh.leaf_bytes(), st));
@@ -324,6 +349,7 @@ void ZkServer::run() {
             J.state = 3;
             J.err = -1;
             slot_busy[s] = false;
+            if (J.big) running_big--;
             in_use -= J.bytes + J.run_bytes;
             fatal = e.what();
             done_cv.notify_all();
@@ -341,10 +367,17 @@ extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes,
         auto srv = std::make_unique<ZkServer>();
         srv->dev = device;
         srv->budget = hbm_budget_bytes;
+        int least = 0, greatest = 0;
+        ZK_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        const int levels[3] = {greatest, (greatest + least) / 2, least};  // high, middle, low
         for (uint32_t i = 0; i < n_slots; i++) {
-            cudaStream_t st;
-            ZK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-            srv->slots.push_back(st);
+            std::vector<cudaStream_t> per;
+            for (int lv : levels) {
+                cudaStream_t st;
+                ZK_CUDA(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, lv));
+                per.push_back(st);
+            }
+            srv->slots.push_back(per);
             srv->slot_busy.push_back(false);
         }
         ZkServer *p = srv.get();
@@ -379,6 +412,10 @@ extern "C" RustError zk_server_submit(ZkServer *srv, const void *host_coeffs, ui
         J->sh = sh;
         J->host_coeffs = host_coeffs;
         J->bytes = sh.leaf_bytes() + sh.digest_bytes() + sh.cap_bytes();
+        // GPU time estimate from the permutation count (about 0.8e9 Poseidon
+        // permutations per second on a B200); only the ordering matters.
+        J->est_s = sh.work() / 0.8e9;
+        J->big = J->est_s > 0.2;
         J->run_bytes = sh.coeff_bytes() + sh.scratch_bytes();
         ZK_CUDA(cudaMallocHost((void **)&J->h_cap, sh.cap_bytes()));
         std::lock_guard<std::mutex> g(srv->mu);
@@ -439,7 +476,7 @@ extern "C" RustError zk_server_release(ZkServer *srv, uint64_t ticket) {
         }
         ZK_CUDA(cudaSetDevice(srv->dev));
         if (J->state == 2) {
-            cudaStream_t st = srv->slots[J->slot];
+            cudaStream_t st = J->stream;
             if (J->d_leaves) ZK_CUDA(cudaFreeAsync(J->d_leaves, st));
             if (J->d_digests) ZK_CUDA(cudaFreeAsync(J->d_digests, st));
             if (J->d_cap) ZK_CUDA(cudaFreeAsync(J->d_cap, st));
@@ -483,14 +520,16 @@ extern "C" RustError zk_server_destroy(ZkServer *srv) {
     if (srv->dispatcher.joinable()) srv->dispatcher.join();
     RustError r = guard([&] {
         ZK_CUDA(cudaSetDevice(srv->dev));
-        for (cudaStream_t st : srv->slots) ZK_CUDA(cudaStreamSynchronize(st));
+        for (auto &per : srv->slots)
+            for (cudaStream_t st : per) ZK_CUDA(cudaStreamSynchronize(st));
         for (auto &kv : srv->jobs) {
             auto &J = *kv.second;
             for (uint64_t *p : {J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch})
                 if (p) cudaFree(p);
             if (J.h_cap) cudaFreeHost(J.h_cap);
         }
-        for (cudaStream_t st : srv->slots) cudaStreamDestroy(st);
+        for (auto &per : srv->slots)
+            for (cudaStream_t st : per) cudaStreamDestroy(st);
     });
     delete srv;
     return r;
