@@ -617,22 +617,21 @@ def run_served(args):
     del bufs, dev_in
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
-    import queue
     import threading
 
     for f in args.rates:
         with zk.Server(hbm_budget_bytes=args.budget_gb << 30, slots=args.streams) as srv:
-            q: queue.Queue = queue.Queue()
-            lat_s = []
+            lat_s, errs = [], []
 
-            def client():
-                while True:
-                    t = q.get()
-                    if t is None:
-                        return
-                    _, l = srv.wait(t)
-                    lat_s.append(l)
-                    srv.release(t)
+            def client():  # collects jobs in completion order and releases their trees at once
+                try:
+                    while len(lat_s) < len(jobs):
+                        t = srv.wait_any(timeout_ms=1000)
+                        if t is not None:
+                            lat_s.append(srv.wait(t)[1])
+                            srv.release(t)
+                except Exception as e:  # noqa: BLE001 - reported by the main thread
+                    errs.append(e)
 
             th = threading.Thread(target=client)
             th.start()
@@ -641,9 +640,10 @@ def run_served(args):
                 now = time.perf_counter() - t0
                 if now < a:
                     time.sleep(a - now)
-                q.put(srv.submit(host[: b << lg].view(b, 1 << lg), r, ch, 0))
-            q.put(None)
+                srv.submit(host[: b << lg].view(b, 1 << lg), r, ch, 0)
             th.join()
+            if errs:
+                raise errs[0]
             span_srv = time.perf_counter() - t0
             st = srv.stats()
         lat, span_plain = plain_res[f]

@@ -194,7 +194,11 @@ ZK_EXTERN RustError zk_commit_batch(const ZkCommitJob *jobs, uint32_t n_jobs, ui
  * caller until the job completes), admitted onto n_slots concurrent streams
  * while leaves + digests + cap of resident trees plus coefficients + scratch of
  * running jobs fit hbm_budget_bytes, and keep their tree on the device until
- * released.  zk_server_wait blocks until the cap is on the host. */
+ * released.  zk_server_wait blocks until the cap is on the host.
+ * zk_server_wait_any returns, in completion order, each job that has finished
+ * (or failed) since the last call, once; *ticket = 0 when nothing is pending or
+ * when timeout_ms passes first (UINT32_MAX waits without limit).  The server
+ * reserves hbm_budget_bytes in the device's memory pool when it is created. */
 typedef struct ZkServer ZkServer;
 typedef struct {
     uint64_t completed, queued, max_queue;
@@ -206,6 +210,7 @@ ZK_EXTERN RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes, 
 ZK_EXTERN RustError zk_server_submit(ZkServer *srv, const void *host_coeffs, uint32_t lg_n, uint32_t rate_bits,
                                      uint32_t batches, uint32_t cap_height, uint32_t hash_type, uint64_t *ticket);
 ZK_EXTERN RustError zk_server_wait(ZkServer *srv, uint64_t ticket, uint64_t *host_cap, double *latency_s);
+ZK_EXTERN RustError zk_server_wait_any(ZkServer *srv, uint32_t timeout_ms, uint64_t *ticket);
 ZK_EXTERN RustError zk_server_result(ZkServer *srv, uint64_t ticket, void **d_leaves, void **d_digests,
                                      void **d_cap);
 ZK_EXTERN RustError zk_server_release(ZkServer *srv, uint64_t ticket);

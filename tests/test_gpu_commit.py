@@ -117,3 +117,44 @@ def test_server_rejects_job_over_budget(zk, oracle):
         with pytest.raises(zk.ZeknoxError):
             srv.wait(t)
         srv.release(t)
+
+
+def test_server_wait_any_returns_each_job_once(zk, oracle):
+    """wait_any hands out every finished ticket exactly once, then None; the
+    caps equal the jobs committed alone."""
+    import torch
+
+    jobs = _mixed_jobs(oracle, 12, 23)
+    want = [zk.commit(_dev(x), r, ch, ht).cap.cpu().numpy() for x, r, ch, ht in jobs]
+    torch.cuda.synchronize()
+    with zk.Server(hbm_budget_bytes=4 << 30, slots=3) as srv:
+        tickets = [srv.submit(x, r, ch, ht) for x, r, ch, ht in jobs]
+        seen = []
+        while len(seen) < len(jobs):
+            t = srv.wait_any(timeout_ms=60000)
+            assert t is not None
+            seen.append(t)
+            cap, _ = srv.wait(t)
+            assert np.array_equal(cap, want[tickets.index(t)])
+            srv.release(t)
+        assert sorted(seen) == sorted(tickets)
+        assert srv.wait_any(timeout_ms=0) is None
+        assert srv.stats()["hbm_in_use"] == 0
+
+
+def test_server_large_job_lane_is_fifo(zk, oracle, monkeypatch):
+    """With every job in the large-job lane (threshold 0 s), jobs run one at a
+    time in arrival order: completions come back in submission order."""
+    import torch
+
+    monkeypatch.setenv("ZK_SERVER_BIG_JOB_S", "0")
+    jobs = _mixed_jobs(oracle, 8, 29)
+    want = [zk.commit(_dev(x), r, ch, ht).cap.cpu().numpy() for x, r, ch, ht in jobs]
+    torch.cuda.synchronize()
+    with zk.Server(hbm_budget_bytes=4 << 30, slots=4) as srv:
+        tickets = [srv.submit(x, r, ch, ht) for x, r, ch, ht in jobs]
+        order = [srv.wait_any(timeout_ms=60000) for _ in jobs]
+        assert order == tickets
+        for t, w in zip(tickets, want):
+            assert np.array_equal(srv.wait(t)[0], w)
+            srv.release(t)

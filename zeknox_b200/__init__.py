@@ -171,6 +171,16 @@ class Server:
         capi.check(capi.LIB.zk_server_wait(self._h, ticket, cap.ctypes.data, ctypes.byref(lat)))
         return cap, lat.value
 
+    def wait_any(self, timeout_ms: int | None = None):
+        """Next completed (or failed) ticket in completion order, each returned once; None when no job is
+        pending or the timeout (milliseconds; None = no limit) passes first."""
+        import ctypes
+
+        t = ctypes.c_uint64()
+        capi.check(capi.LIB.zk_server_wait_any(self._h, 0xFFFFFFFF if timeout_ms is None else int(timeout_ms),
+                                               ctypes.byref(t)))
+        return t.value or None
+
     def result_ptrs(self, ticket: int):
         import ctypes
 

@@ -172,17 +172,21 @@ __device__ __forceinline__ uint64_t pr_mul(uint64_t a, uint64_t b) {
 }
 
 // a * b + c (a, b any u64; c < 2^68 given as (c_lo, c_hi)); partially reduced.
+// (a b + c <= (2^64-1)^2 + 2^68 < 2^128, so the sum does not wrap.)
 __device__ __forceinline__ uint64_t pr_mul_add(uint64_t a, uint64_t b, uint64_t c_lo, uint32_t c_hi) {
-    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
-    const uint64_t p00 = (uint64_t)a0 * b0;
-    const uint64_t t = (uint64_t)a0 * b1 + (p00 >> 32);
-    const uint64_t u = (uint64_t)a1 * b0 + (uint32_t)t;
-    uint64_t v = (uint64_t)a1 * b1 + (t >> 32) + (u >> 32);
-    const uint64_t lo = ((uint64_t)(uint32_t)u << 32) | (uint32_t)p00;
-    // (v:lo) + (c_hi:c_lo) <= (2^64-1)^2 + 2^68 < 2^128
-    const uint64_t s = lo + c_lo;
-    v += (uint64_t)c_hi + (s < lo ? 1u : 0u);
-    return pr_reduce128((uint32_t)s, (uint32_t)(s >> 32), (uint32_t)v, (uint32_t)(v >> 32));
+    uint64_t lo, hi;
+    mul_wide(a, b, lo, hi);
+    uint32_t r0, r1, r2, r3;
+    asm("{\n\t"
+        "add.cc.u32  %0, %4, %8;\n\t"
+        "addc.cc.u32 %1, %5, %9;\n\t"
+        "addc.cc.u32 %2, %6, %10;\n\t"
+        "addc.u32    %3, %7, 0;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+        : "r"((uint32_t)lo), "r"((uint32_t)(lo >> 32)), "r"((uint32_t)hi), "r"((uint32_t)(hi >> 32)),
+          "r"((uint32_t)c_lo), "r"((uint32_t)(c_lo >> 32)), "r"(c_hi));
+    return pr_reduce128(r0, r1, r2, r3);
 }
 
 // a + c for any u64 a and c < p: one wrap at most, fixed by adding EPS.
@@ -199,7 +203,8 @@ __device__ __forceinline__ uint64_t pr_pow7(uint64_t x) {
     return pr_mul(x3, x4);
 }
 
-// al + ah * 2^32 + c for al, ah < 2^60 and any c < 2^64; partially reduced.
+// al + ah * 2^32 + c for any al, c < 2^64 and ah < 2^64 - 2^33; partially
+// reduced.
 __device__ __forceinline__ uint64_t pr_reduce_split(uint64_t al, uint64_t ah, uint64_t c) {
     uint32_t r0, r1;
     asm("{\n\t"

@@ -18,51 +18,128 @@
 
 namespace zk {
 
-__constant__ uint64_t c_poseidon_rc[360] = {ZK_POSEIDON_RC_LIST};
-__constant__ uint64_t c_poseidon2_rc[360] = {ZK_POSEIDON2_RC_LIST};
+// ---------------------------------------------------- exact FP64 layers
+// The linear layers of both Poseidon variants have small non-negative integer
+// coefficients.  They run on the FP64 pipe (full rate on sm_100), next to the
+// integer pipes that carry the S-box products: each lane is split into its two
+// 32-bit halves, each half-vector goes through the layer in doubles, and every
+// product and partial sum is an integer (or half-integer) far below 2^53, so
+// the FP64 arithmetic is exact.
+//
+// No int<->double conversion instruction is used.  A 32-bit x enters as the
+// double whose bit pattern is 0x43300000:x, which is 2^52 + x; a result v
+// (0 <= v < 2^41) leaves as the double 2^52 + v, whose bit pattern is
+// kMagicBits + v.  Those two offsets are cancelled by subtracting
+// kMagicAdj = kMagicBits * (1 + 2^32) mod p from the constant that is added
+// in the same reduction (the next round's constants), so the constant tables
+// used there are stored pre-adjusted.
+constexpr double kMagic = 4503599627370496.0;  // 2^52
+constexpr uint64_t kMagicBits = 0x4330000000000000ull;
+__host__ __device__ constexpr uint64_t cx_canon(uint64_t a) { return a >= ZK_P ? a - ZK_P : a; }
+constexpr uint64_t cx_add_mod(uint64_t a, uint64_t b) {  // a, b < p
+    return a >= ZK_P - b ? a - (ZK_P - b) : a + b;
+}
+constexpr uint64_t cx_sub_mod(uint64_t a, uint64_t b) { return a >= b ? a - b : a + (ZK_P - b); }
+// kMagicBits * 2^32 = hi32 * 2^64 = hi32 * (2^32 - 1) (mod p) because its low word is zero.
+constexpr uint64_t kMagicAdj = cx_add_mod(kMagicBits, (kMagicBits >> 32 << 32) - (kMagicBits >> 32));
+static_assert((kMagicBits & 0xffffffffull) == 0 && kMagicAdj == 0x865fffffbcd00000ull, "magic constants");
+constexpr uint64_t kMagicNeg = cx_sub_mod(0, kMagicAdj);  // added where no constant follows
+
+struct RcTable {
+    uint64_t v[360];
+};
+constexpr RcTable magic_adjusted(RcTable t) {
+    for (int i = 0; i < 360; i++) t.v[i] = cx_sub_mod(cx_canon(t.v[i]), kMagicAdj);
+    return t;
+}
+
+__constant__ uint64_t c_poseidon2_rc[360] = {ZK_POSEIDON2_RC_LIST};  // internal layer
+__constant__ RcTable c_poseidon_rcm = magic_adjusted(RcTable{{ZK_POSEIDON_RC_LIST}});
+__constant__ RcTable c_poseidon2_rcm = magic_adjusted(RcTable{{ZK_POSEIDON2_RC_LIST}});
+__constant__ RcTable c_poseidon_rc = RcTable{{ZK_POSEIDON_RC_LIST}};  // round 0 is added before the first S-box
 __constant__ uint64_t c_poseidon2_diag[12] = {ZK_POSEIDON2_DIAG_LIST};
 __constant__ uint64_t c_keccak_rc[24] = {ZK_KECCAK_RC_LIST};
 
-// out = M * x (+ c) for a 12x12 matrix of small non-negative integer
-// coefficients (row sums < 2^9).  The 32-bit halves of x are converted to
-// doubles and each row is accumulated with FP64 multiply-adds: every product
-// and partial sum is an integer below 276 * 2^32 < 2^41 < 2^53, so the FP64
-// arithmetic is exact.  This moves the 288 multiply-adds of a layer onto the
-// FP64 pipe (full rate on sm_100), next to the integer pipes that carry the
-// S-box products.  Each row is then reduced once, adding c[r] (the next
-// round's constants; c == nullptr adds nothing).  Inputs and outputs are
-// partially reduced.  coef(r, c) must be a constant expression after unrolling.
-template <class Coef>
-__device__ __forceinline__ void small_matvec12(uint64_t s[12], Coef coef, const uint64_t *c) {
-    double lo[12], hi[12];
+__device__ __forceinline__ double magic_in(uint32_t x) { return __hiloint2double(0x43300000, (int)x); }
+__device__ __forceinline__ uint64_t magic_out(double v) { return (uint64_t)__double_as_longlong(v); }
+
+// s[r] <- (lo[r] + hi[r] * 2^32 + c[r]) mod p (partially reduced), where lo, hi
+// are the magic-offset outputs of a layer and cm the adjusted constants
+// (nullptr: no constant).
+__device__ __forceinline__ void magic_combine(uint64_t s[12], const double lo[12], const double hi[12],
+                                              const uint64_t *cm) {
 #pragma unroll
-    for (int i = 0; i < 12; i++) {
-        lo[i] = __uint2double_rn((uint32_t)s[i]);
-        hi[i] = __uint2double_rn((uint32_t)(s[i] >> 32));
-    }
-#pragma unroll
-    for (int r = 0; r < 12; r++) {
-        double al = 0.0, ah = 0.0;
-#pragma unroll
-        for (int k = 0; k < 12; k++) {
-            const uint32_t m = coef(r, k);
-            if (m) {
-                al = fma((double)m, lo[k], al);
-                ah = fma((double)m, hi[k], ah);
-            }
-        }
-        s[r] = pr_reduce_split(__double2ull_rz(al), __double2ull_rz(ah), c ? c[r] : 0ull);
-    }
+    for (int r = 0; r < 12; r++) s[r] = pr_reduce_split(magic_out(lo[r]), magic_out(hi[r]), cm ? cm[r] : kMagicNeg);
 }
 
 // ------------------------------------------------------------ Poseidon
-struct PoseidonMds {
-    __device__ __forceinline__ uint32_t operator()(int r, int c) const {
-        constexpr uint32_t circ[12] = {ZK_POSEIDON_MDS_CIRC_LIST};
-        constexpr uint32_t diag[12] = {ZK_POSEIDON_MDS_DIAG_LIST};
-        return circ[(c - r + 12) % 12] + (r == c ? diag[r] : 0u);
+// MDS = C + diag(8, 0, ..., 0), C circulant with C[r][k] = circ[(k - r) mod 12].
+// In 6x6 blocks C = [[A, B], [B, A]], so with u = x_lo + x_hi, w = x_lo - x_hi
+// (x_lo = lanes 0-5, x_hi = lanes 6-11):
+//   2 (C x)_lo = (A + B) u + (A - B) w,   2 (C x)_hi = (A + B) u - (A - B) w,
+// which takes 72 multiply-adds per half-vector instead of 144.
+#define ZK_MDS_TABLES                                                  \
+    constexpr uint32_t circ[12] = {ZK_POSEIDON_MDS_CIRC_LIST};         \
+    constexpr uint32_t diag[12] = {ZK_POSEIDON_MDS_DIAG_LIST};
+constexpr bool diag_only_lane0() {
+    ZK_MDS_TABLES
+    for (int i = 1; i < 12; i++)
+        if (diag[i]) return false;
+    return circ[0] > 0;
+}
+static_assert(diag_only_lane0(), "the MDS layer below assumes diag(d, 0, ..., 0)");
+__host__ __device__ constexpr int mds_diag0() {
+    ZK_MDS_TABLES
+    return (int)diag[0] + 0 * (int)circ[0];
+}
+__host__ __device__ constexpr int mds_p2(int r, int k) {  // A + B, plus d on (0, 0)
+    ZK_MDS_TABLES
+    return (int)(circ[(k - r + 12) % 12] + circ[(k + 6 - r + 12) % 12]) + (r == 0 && k == 0 ? (int)diag[0] : 0);
+}
+__host__ __device__ constexpr int mds_q2(int r, int k) {  // A - B, plus d on (0, 0)
+    ZK_MDS_TABLES
+    return (int)circ[(k - r + 12) % 12] - (int)circ[(k + 6 - r + 12) % 12] + (r == 0 && k == 0 ? (int)diag[0] : 0);
+}
+#undef ZK_MDS_TABLES
+
+// One half-vector: a[i] = 2^52 + x[i] in, o[r] = 2^52 + (MDS x)[r] out.
+__device__ __forceinline__ void poseidon_mds_half(const double a[12], double o[12]) {
+    double u[6], w[6], x6 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        const double t = a[i + 6] - kMagic;  // x_hi[i]
+        if (i == 0) x6 = t;
+        w[i] = a[i] - a[i + 6];              // exact: both in [2^52, 2^53)
+        u[i] = fma(2.0, t, w[i]);
     }
-};
+#pragma unroll
+    for (int r = 0; r < 6; r++) {
+        double pa = (double)mds_p2(r, 0) * u[0], qa = (double)mds_q2(r, 0) * w[0];
+#pragma unroll
+        for (int k = 1; k < 6; k++) {
+            pa = fma((double)mds_p2(r, k), u[k], pa);
+            qa = fma((double)mds_q2(r, k), w[k], qa);
+        }
+        // The (0, 0) terms carry d (u + w) = 2 d x_lo[0] into lane 0; lane 6
+        // must not get d (u - w) = 2 d x_hi[0], so it is taken out again.
+        double d = pa - qa;
+        if (r == 0) d = fma(-2.0 * (double)mds_diag0(), x6, d);
+        o[r] = fma(0.5, pa + qa, kMagic);
+        o[r + 6] = fma(0.5, d, kMagic);
+    }
+}
+
+// s <- MDS s + c (c: the adjusted constants of the next round, or nullptr).
+__device__ __forceinline__ void poseidon_mds(uint64_t s[12], const uint64_t *cm) {
+    double a[12], lo[12], hi[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) a[i] = magic_in((uint32_t)s[i]);
+    poseidon_mds_half(a, lo);
+#pragma unroll
+    for (int i = 0; i < 12; i++) a[i] = magic_in((uint32_t)(s[i] >> 32));
+    poseidon_mds_half(a, hi);
+    magic_combine(s, lo, hi, cm);
+}
 
 // x^7 on all 12 lanes, as three passes over 4 lanes with a rotation between
 // them (keeps the loop body, and so the instruction footprint, small).
@@ -87,24 +164,54 @@ __device__ __forceinline__ void pow7_all(uint64_t s[12]) {
 // added inside the previous round's MDS reduction.
 __device__ __forceinline__ void poseidon_permute(uint64_t s[12]) {
 #pragma unroll
-    for (int i = 0; i < 12; i++) s[i] = pr_add_c(s[i], c_poseidon_rc[i]);
+    for (int i = 0; i < 12; i++) s[i] = pr_add_c(s[i], c_poseidon_rc.v[i]);
 #pragma unroll 1
     for (int rnd = 0; rnd < 30; rnd++) {
         if (rnd < 4 || rnd >= 26) pow7_all(s);
         else s[0] = pr_pow7(s[0]);
-        small_matvec12(s, PoseidonMds(), rnd < 29 ? &c_poseidon_rc[12 * (rnd + 1)] : nullptr);
+        poseidon_mds(s, rnd < 29 ? &c_poseidon_rcm.v[12 * (rnd + 1)] : nullptr);
     }
 }
 
 // ----------------------------------------------------------- Poseidon2
 // External layer = (I + [1 1 1] (x) I_4) * blockdiag(M4, M4, M4) with
-// M4 = [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]] (poseidon2.cu:64-110).
-struct Poseidon2External {
-    __device__ __forceinline__ uint32_t operator()(int r, int c) const {
-        constexpr uint32_t m4[16] = {5, 7, 1, 3, 4, 6, 1, 1, 1, 3, 5, 7, 1, 1, 4, 6};
-        return m4[(r & 3) * 4 + (c & 3)] * ((r >> 2) == (c >> 2) ? 2u : 1u);
+// M4 = [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]] (poseidon2.cu:64-110):
+// y_b = M4 x_b per 4-lane block, then out_b = y_b + (y_0 + y_1 + y_2).
+// M4 x is the 8-addition network of the Poseidon2 paper (Grassi, Khovratovich,
+// Schofnegger 2023, section 5.1): t0 = x0 + x1, t1 = x2 + x3, t2 = 2 x1 + t1,
+// t3 = 2 x3 + t0, t4 = 4 t1 + t3, t5 = 4 t0 + t2, M4 x = (t3 + t5, t5, t2 + t4, t4).
+__device__ __forceinline__ void poseidon2_external_half(const double a[12], double o[12]) {
+    double y[12];
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+        const double x0 = a[4 * b] - kMagic, x1 = a[4 * b + 1] - kMagic;
+        const double x2 = a[4 * b + 2] - kMagic, x3 = a[4 * b + 3] - kMagic;
+        const double t0 = x0 + x1, t1 = x2 + x3;
+        const double t2 = fma(2.0, x1, t1), t3 = fma(2.0, x3, t0);
+        const double t4 = fma(4.0, t1, t3), t5 = fma(4.0, t0, t2);
+        y[4 * b] = t3 + t5;
+        y[4 * b + 1] = t5;
+        y[4 * b + 2] = t2 + t4;
+        y[4 * b + 3] = t4;
     }
-};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const double sm = (y[j] + y[4 + j]) + (y[8 + j] + kMagic);
+#pragma unroll
+        for (int b = 0; b < 3; b++) o[4 * b + j] = y[4 * b + j] + sm;
+    }
+}
+
+__device__ __forceinline__ void poseidon2_external(uint64_t s[12], const uint64_t *cm) {
+    double a[12], lo[12], hi[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) a[i] = magic_in((uint32_t)s[i]);
+    poseidon2_external_half(a, lo);
+#pragma unroll
+    for (int i = 0; i < 12; i++) a[i] = magic_in((uint32_t)(s[i] >> 32));
+    poseidon2_external_half(a, hi);
+    magic_combine(s, lo, hi, cm);
+}
 
 // x_i <- x_i * D_i + sum_j x_j (+ next round's constants): poseidon2.cu:131-146.
 __device__ __forceinline__ void poseidon2_internal(uint64_t s[12], const uint64_t *c) {
@@ -125,11 +232,11 @@ __device__ __forceinline__ void poseidon2_internal(uint64_t s[12], const uint64_
 }
 
 __device__ __forceinline__ void poseidon2_permute(uint64_t s[12]) {
-    small_matvec12(s, Poseidon2External(), &c_poseidon2_rc[0]);
+    poseidon2_external(s, &c_poseidon2_rcm.v[0]);
 #pragma unroll 1
     for (int rnd = 0; rnd < 4; rnd++) {
         pow7_all(s);
-        small_matvec12(s, Poseidon2External(), &c_poseidon2_rc[12 * (rnd + 1)]);
+        poseidon2_external(s, &c_poseidon2_rcm.v[12 * (rnd + 1)]);
     }
     // internal rounds: only lane 0 of their constants is non-zero
 #pragma unroll 1
@@ -140,7 +247,7 @@ __device__ __forceinline__ void poseidon2_permute(uint64_t s[12]) {
 #pragma unroll 1
     for (int rnd = 26; rnd < 30; rnd++) {
         pow7_all(s);
-        small_matvec12(s, Poseidon2External(), rnd < 29 ? &c_poseidon2_rc[12 * (rnd + 1)] : nullptr);
+        poseidon2_external(s, rnd < 29 ? &c_poseidon2_rcm.v[12 * (rnd + 1)] : nullptr);
     }
 }
 

@@ -10,17 +10,22 @@
 //
 // ZkServer: a request loop for commits that arrive over time.  A dispatcher
 // thread admits queued jobs onto free slots while their device memory fits an
-// HBM budget; admitted jobs run concurrently.  Admission is shortest-job-first
-// with aging (a job's estimated GPU time minus half the time it has waited),
-// at most one large job runs at a time (two large trees sharing the GPU only
-// delay each other), and each job's stream gets a CUDA priority by size, so
-// small commits are scheduled onto SMs ahead of the blocks of a large one
-// that is already running.  The tree (leaves + digests + cap) of every job
-// stays resident on the device until the client releases it; the cap is also
-// copied to the host.  Latency (submit to completion of the cap copy) is
-// recorded for p50 / p99.
+// HBM budget (reserved in the device's memory pool when the server starts, so
+// an admitted job never waits for physical memory); admitted jobs run
+// concurrently.  Jobs are split by estimated GPU time into two lanes.  Small
+// jobs are admitted shortest-first with aging (estimated time minus half the
+// time waited).  Large jobs are admitted in arrival order, one at a time (two
+// large trees sharing the GPU only delay each other), and while the oldest
+// large job waits for memory, small jobs are admitted only if they leave room
+// for it.  Each job's stream gets a CUDA priority by size, so the blocks of
+// small commits are scheduled onto SMs ahead of those of a large one that is
+// already running.  The tree (leaves + digests + cap) of every job stays
+// resident on the device until the client releases it; the cap is also copied
+// to the host.  Completions are queued in order for zk_server_wait_any.
+// Latency (submit to completion of the cap copy) is recorded for p50 / p99.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -213,11 +218,13 @@ struct ZkServer {
         double est_s = 0;           // estimated GPU time
         cudaStream_t stream = nullptr;  // the stream the job ran on
         bool big = false;
+        uint64_t seq = 0;           // submission order
         int state = 0;              // 0 queued, 1 running, 2 done, 3 failed
         int err = 0;
     };
     int dev = 0;
     uint64_t budget = 0, in_use = 0, peak = 0;
+    double big_s = 0.2;  // jobs estimated above this many GPU seconds take the large-job lane
     std::vector<std::vector<cudaStream_t>> slots;  // [slot][priority level]: level 0 highest
     std::vector<bool> slot_busy;
     int running_big = 0;
@@ -225,6 +232,8 @@ struct ZkServer {
     std::condition_variable cv;        // dispatcher wake-up
     std::condition_variable done_cv;   // completions
     std::deque<uint64_t> queue;
+    std::deque<uint64_t> done_q;       // completed or failed, not yet returned by wait_any
+    uint64_t n_running = 0;
     std::unordered_map<uint64_t, std::unique_ptr<Job>> jobs;
     uint64_t next_ticket = 1;
     bool stop = false;
@@ -257,6 +266,8 @@ void CUDART_CB on_done(void *p) {
     J.state = 2;
     srv->slot_busy[J.slot] = false;
     if (J.big) srv->running_big--;
+    srv->n_running--;
+    srv->done_q.push_back(d->ticket);
     srv->in_use -= J.run_bytes;  // coeffs + scratch were freed on the stream before this point
     srv->latencies.push_back(std::chrono::duration<double>(J.t_done - J.t_submit).count());
     srv->elems_done += (double)J.sh.N() * J.sh.batches;
@@ -284,32 +295,39 @@ void ZkServer::run() {
             if (J.bytes + J.run_bytes > budget) {
                 J.state = 3;
                 J.err = (int)cudaErrorMemoryAllocation;
+                done_q.push_back(*it);
                 done_cv.notify_all();
                 it = queue.erase(it);
             } else {
                 ++it;
             }
         }
-        // Then the queued job that fits now with the smallest estimated GPU
-        // time minus half its waiting time (shortest-job-first with aging); a
-        // large job waits while another large job runs, unless nothing else can go.
-        auto pick = queue.end(), pick_big = queue.end();
-        double best = 1e300, best_big = 1e300;
-        const auto now = std::chrono::steady_clock::now();
+        // The oldest large job goes next when no other large job runs and it
+        // fits; otherwise the small job with the smallest estimated time minus
+        // half its waiting time (shortest-job-first with aging) that fits and,
+        // while that large job waits for memory, leaves room for it.
+        auto pick = queue.end(), big_head = queue.end();
         for (auto it = queue.begin(); it != queue.end(); ++it) {
             const Job &J = *jobs[*it];
-            if (in_use + J.bytes + J.run_bytes > budget) continue;
-            const double key = J.est_s - 0.5 * std::chrono::duration<double>(now - J.t_submit).count();
-            if (J.big && running_big > 0) {
-                if (key < best_big) best_big = key, pick_big = it;
-                continue;
-            }
-            if (key < best) best = key, pick = it;
+            if (J.big && (big_head == queue.end() || J.seq < jobs[*big_head]->seq)) big_head = it;
         }
-        if (pick == queue.end() && pick_big != queue.end() &&
-            std::find(slot_busy.begin(), slot_busy.end(), true) == slot_busy.end())
-            pick = pick_big;  // the GPU is idle: run it anyway
-        if (pick == queue.end()) {  // nothing fits until memory is released
+        uint64_t reserve = 0;
+        if (big_head != queue.end() && running_big == 0) {
+            const Job &B = *jobs[*big_head];
+            if (in_use + B.bytes + B.run_bytes <= budget) pick = big_head;
+            else reserve = B.bytes + B.run_bytes;
+        }
+        if (pick == queue.end()) {
+            double best = 1e300;
+            const auto now = std::chrono::steady_clock::now();
+            for (auto it = queue.begin(); it != queue.end(); ++it) {
+                const Job &J = *jobs[*it];
+                if (J.big || in_use + J.bytes + J.run_bytes + reserve > budget) continue;
+                const double key = J.est_s - 0.5 * std::chrono::duration<double>(now - J.t_submit).count();
+                if (key < best) best = key, pick = it;
+            }
+        }
+        if (pick == queue.end()) {  // nothing can go until a job completes or memory is released
             cv.wait(lk);
             continue;
         }
@@ -321,6 +339,7 @@ void ZkServer::run() {
         J.slot = s;
         J.state = 1;
         if (J.big) running_big++;
+        n_running++;
         in_use += J.bytes + J.run_bytes;
         peak = std::max(peak, in_use);
         lk.unlock();
@@ -350,6 +369,8 @@ void ZkServer::run() {
             J.err = -1;
             slot_busy[s] = false;
             if (J.big) running_big--;
+            n_running--;
+            done_q.push_back(t);
             in_use -= J.bytes + J.run_bytes;
             fatal = e.what();
             done_cv.notify_all();
@@ -367,6 +388,8 @@ extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes,
         auto srv = std::make_unique<ZkServer>();
         srv->dev = device;
         srv->budget = hbm_budget_bytes;
+        // ZK_SERVER_BIG_JOB_S overrides the large-job threshold (seconds of estimated GPU time).
+        if (const char *e = getenv("ZK_SERVER_BIG_JOB_S")) srv->big_s = atof(e);
         int least = 0, greatest = 0;
         ZK_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         const int levels[3] = {greatest, (greatest + least) / 2, least};  // high, middle, low
@@ -379,6 +402,19 @@ extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes,
             }
             srv->slots.push_back(per);
             srv->slot_busy.push_back(false);
+        }
+        // Reserve the budget in the pool (which keeps freed memory: its release
+        // threshold is unlimited), so admitted jobs are served from mapped
+        // memory.  If the device cannot hold it all now, jobs grow the pool.
+        {
+            cudaStream_t st = srv->slots[0][0];
+            void *p = nullptr;
+            if (cudaMallocAsync(&p, hbm_budget_bytes, st) == cudaSuccess) {
+                ZK_CUDA(cudaFreeAsync(p, st));
+                ZK_CUDA(cudaStreamSynchronize(st));
+            } else {
+                cudaGetLastError();
+            }
         }
         ZkServer *p = srv.get();
         srv->dispatcher = std::thread([p] {
@@ -415,12 +451,13 @@ extern "C" RustError zk_server_submit(ZkServer *srv, const void *host_coeffs, ui
         // GPU time estimate from the permutation count (about 0.8e9 Poseidon
         // permutations per second on a B200); only the ordering matters.
         J->est_s = sh.work() / 0.8e9;
-        J->big = J->est_s > 0.2;
+        J->big = J->est_s > srv->big_s;
         J->run_bytes = sh.coeff_bytes() + sh.scratch_bytes();
         ZK_CUDA(cudaMallocHost((void **)&J->h_cap, sh.cap_bytes()));
         std::lock_guard<std::mutex> g(srv->mu);
         require(srv->fatal.empty(), "server failed: " + srv->fatal);
         J->ticket = srv->next_ticket++;
+        J->seq = J->ticket;
         J->t_submit = std::chrono::steady_clock::now();
         if (!srv->any) {
             srv->t_first = J->t_submit;
@@ -446,6 +483,24 @@ extern "C" RustError zk_server_wait(ZkServer *srv, uint64_t ticket, uint64_t *ho
                                                                           : "job failed: " + srv->fatal);
         if (host_cap) memcpy(host_cap, J->h_cap, J->sh.cap_bytes());
         if (latency_s) *latency_s = std::chrono::duration<double>(J->t_done - J->t_submit).count();
+    });
+}
+
+extern "C" RustError zk_server_wait_any(ZkServer *srv, uint32_t timeout_ms, uint64_t *ticket) {
+    return guard([&] {
+        require(srv != nullptr && ticket != nullptr, "null argument");
+        *ticket = 0;
+        std::unique_lock<std::mutex> lk(srv->mu);
+        auto ready = [&] {
+            while (!srv->done_q.empty() && !srv->jobs.count(srv->done_q.front())) srv->done_q.pop_front();
+            return !srv->done_q.empty() || (srv->queue.empty() && srv->n_running == 0) || !srv->fatal.empty();
+        };
+        if (timeout_ms == UINT32_MAX) srv->done_cv.wait(lk, ready);
+        else srv->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready);
+        if (!srv->done_q.empty() && srv->jobs.count(srv->done_q.front())) {
+            *ticket = srv->done_q.front();
+            srv->done_q.pop_front();
+        }
     });
 }
 
@@ -530,6 +585,9 @@ extern "C" RustError zk_server_destroy(ZkServer *srv) {
         }
         for (auto &per : srv->slots)
             for (cudaStream_t st : per) cudaStreamDestroy(st);
+        // Hand the reserved budget back to the device.
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, srv->dev) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     });
     delete srv;
     return r;
