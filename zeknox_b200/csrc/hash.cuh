@@ -214,20 +214,26 @@ __device__ __forceinline__ void poseidon2_external(uint64_t s[12], const uint64_
 }
 
 // x_i <- x_i * D_i + sum_j x_j (+ next round's constants): poseidon2.cu:131-146.
+// The sum of the 12 lanes is kept exact in 96 bits (carry chain).
 __device__ __forceinline__ void poseidon2_internal(uint64_t s[12], const uint64_t *c) {
-    uint64_t sl = s[0];
-    uint32_t sh = 0;
+    uint32_t s0 = (uint32_t)s[0], s1 = (uint32_t)(s[0] >> 32), s2 = 0;
 #pragma unroll
     for (int i = 1; i < 12; i++) {
-        const uint64_t t = sl + s[i];
-        sh += t < sl ? 1u : 0u;
-        sl = t;
+        asm("add.cc.u32 %0, %0, %3;\n\t"
+            "addc.cc.u32 %1, %1, %4;\n\t"
+            "addc.u32 %2, %2, 0;"
+            : "+r"(s0), "+r"(s1), "+r"(s2)
+            : "r"((uint32_t)s[i]), "r"((uint32_t)(s[i] >> 32)));
     }
 #pragma unroll
     for (int i = 0; i < 12; i++) {
-        const uint64_t cl = sl + c[i];
-        const uint32_t ch = sh + (cl < sl ? 1u : 0u);
-        s[i] = pr_mul_add(s[i], c_poseidon2_diag[i], cl, ch);
+        uint32_t c0, c1, c2;
+        asm("add.cc.u32 %0, %3, %6;\n\t"
+            "addc.cc.u32 %1, %4, %7;\n\t"
+            "addc.u32 %2, %5, 0;"
+            : "=r"(c0), "=r"(c1), "=r"(c2)
+            : "r"(s0), "r"(s1), "r"(s2), "r"((uint32_t)c[i]), "r"((uint32_t)(c[i] >> 32)));
+        s[i] = pr_mul_add(s[i], c_poseidon2_diag[i], ((uint64_t)c1 << 32) | c0, c2);
     }
 }
 

@@ -65,7 +65,11 @@ constexpr int kTile = 128;
 __device__ __forceinline__ uint64_t *node_ptr(uint64_t *sub, uint64_t w, uint64_t i) { return sub + 4 * (w - 2 + i); }
 
 // Block = tile of blockDim.x (<= 128, a power of two) consecutive leaves of one
-// subtree.  Hashes the leaves, then folds log2(blockDim.x) levels.
+// subtree.  Hashes the leaves, then folds log2(blockDim.x) levels.  For the
+// Poseidon hashers a node is the sponge of its two children's 8 words (the
+// same state as hash_two), so leaves and nodes go through one call site of
+// the permutation: one copy of its code in the kernel, which keeps the
+// instruction working set of the resident warps small.
 template <int H>
 __global__ void __launch_bounds__(kTile) merkle_tile(const uint64_t *__restrict__ leaves, uint32_t leaf_size,
                                                      uint64_t *__restrict__ digests, uint64_t *__restrict__ cap,
@@ -75,29 +79,55 @@ __global__ void __launch_bounds__(kTile) merkle_tile(const uint64_t *__restrict_
     const uint64_t leaf = blockIdx.x * (uint64_t)T + t;
     const uint64_t sub = leaf / ls, j0 = (blockIdx.x * (uint64_t)T) % ls;
     uint64_t *base = digests + 4 * sub * ds;
-    uint64_t d[4];
-    hash_one<H>(leaves + leaf * leaf_size, leaf_size, d);
-    uint64_t *dst = base + 4 * (ds - ls + j0 + t);
+    if constexpr (H == kKeccak) {
+        uint64_t d[4];
+        hash_one<H>(leaves + leaf * leaf_size, leaf_size, d);
+        uint64_t *dst = base + 4 * (ds - ls + j0 + t);
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        dst[k] = d[k];
-        sm[4 * t + k] = d[k];
-    }
-    uint64_t w = ls;
-    for (uint32_t active = T >> 1; active >= 1; active >>= 1) {
-        w >>= 1;
-        __syncthreads();
-        uint64_t h[4];
-        if (t < active) hash_two<H>(&sm[8 * t], &sm[8 * t + 4], h);
-        __syncthreads();
-        if (t < active) {
-            const uint64_t i = (j0 >> (__ffs(T / active) - 1)) + t;  // index in the level of width w
-            uint64_t *o = w >= 2 ? node_ptr(base, w, i) : cap + 4 * sub;
+        for (int k = 0; k < 4; k++) {
+            dst[k] = d[k];
+            sm[4 * t + k] = d[k];
+        }
+        uint64_t w = ls;
+        for (uint32_t active = T >> 1; active >= 1; active >>= 1) {
+            w >>= 1;
+            __syncthreads();
+            uint64_t h[4];
+            if (t < active) hash_two<H>(&sm[8 * t], &sm[8 * t + 4], h);
+            __syncthreads();
+            if (t < active) {
+                const uint64_t i = (j0 >> (__ffs(T / active) - 1)) + t;  // index in the level of width w
+                uint64_t *o = w >= 2 ? node_ptr(base, w, i) : cap + 4 * sub;
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                o[k] = h[k];
-                sm[4 * t + k] = h[k];
+                for (int k = 0; k < 4; k++) {
+                    o[k] = h[k];
+                    sm[4 * t + k] = h[k];
+                }
             }
+        }
+    } else {
+        const uint64_t *src = leaves + leaf * leaf_size;
+        uint32_t n = leaf_size, active = T, lvl = 0;
+        for (;;) {
+            uint64_t h[4];
+            if (t < active) hash_one<H>(src, n, h);
+            if (lvl) __syncthreads();  // every child in sm has been read
+            if (t < active) {
+                const uint64_t w = ls >> lvl;  // width of this level
+                uint64_t *o = lvl == 0 ? base + 4 * (ds - ls + j0 + t)
+                                       : (w >= 2 ? node_ptr(base, w, (j0 >> lvl) + t) : cap + 4 * sub);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    o[k] = h[k];
+                    sm[4 * t + k] = h[k];
+                }
+            }
+            active >>= 1;
+            if (!active) break;
+            __syncthreads();
+            src = &sm[8 * t];
+            n = 8;
+            lvl++;
         }
     }
 }
