@@ -70,6 +70,21 @@ def test_lde_device_buffers_and_directions(zk, oracle, lg_n, rate, batches, inve
     assert np.array_equal(_host(d_in), x)  # input untouched
 
 
+@pytest.mark.parametrize("in_dev,out_dev,batches", [(False, False, 19), (False, True, 33), (True, False, 16),
+                                                     (False, False, 135)])
+def test_lde_grouped_host_copies(zk, oracle, in_dev, out_dev, batches):
+    """Host buffers with >= 16 polynomials go through the grouped copy/compute
+    pipeline (uneven last group included); the result is the same LDE."""
+    lg_n, rate = 9, 2
+    x = oracle.field_elems(4000 + batches, batches << lg_n)
+    exp = oracle.batch_lde(x, lg_n, rate, batches)
+    src = _dev(x) if in_dev else x
+    out = _dev(np.zeros(batches << (lg_n + rate), dtype=np.uint64)) if out_dev else np.zeros_like(exp)
+    zk.lde_batch(0, out.data_ptr() if out_dev else out.ctypes.data, src.data_ptr() if in_dev else src.ctypes.data,
+                 lg_n, _cfg(zk, batches, rate, in_dev, out_dev, True))
+    assert np.array_equal(_host(out) if out_dev else out, exp)
+
+
 def test_lde_mixed_host_device(zk, oracle):
     lg_n, rate, b = 11, 2, 3
     x = oracle.field_elems(3, b << lg_n)

@@ -6,8 +6,10 @@
 #include <string.h>
 #include <time.h>
 
+#include <algorithm>
 #include <exception>
 #include <string>
+#include <vector>
 
 #include "../../include/zeknox.h"
 #include "merkle.cuh"
@@ -254,7 +256,6 @@ extern "C" RustError compute_batched_lde(size_t device_id, void *output, void *i
         uint64_t *d_out = (uint64_t *)output;
         if (!cfg.are_inputs_on_device) {
             sin.alloc(in_total * sizeof(uint64_t), s);
-            h2d(sin.p, input, in_total * sizeof(uint64_t), s);
             d_in = sin.as<uint64_t>();
         }
         if (!cfg.are_outputs_on_device) {
@@ -263,10 +264,56 @@ extern "C" RustError compute_batched_lde(size_t device_id, void *output, void *i
         }
         require(!(cfg.are_inputs_on_device && cfg.are_outputs_on_device && (const void *)d_in == (void *)d_out),
                 "input and output must not alias");
-        lde_device(ctx, d_out, d_in, lg_n, rb, cfg.batches, ntt_direction == inverse, cfg.with_coset, s);
-        if (cfg.salt_size) salt_run(d_out + (uint64_t)cfg.batches * N, (uint64_t)cfg.salt_size * N, seed_now(), s);
-        if (!cfg.are_outputs_on_device) d2h(output, d_out, out_total * sizeof(uint64_t), s);
-        ZK_CUDA(cudaStreamSynchronize(s));
+        // Host buffers: polynomials go in groups, so that the copy of one group
+        // overlaps the transform of another (copies on the context's copy stream).
+        const uint64_t B = cfg.batches;
+        const uint64_t groups = (cfg.are_inputs_on_device && cfg.are_outputs_on_device) || B < 16 ? 1 : 4;
+        const uint64_t gsz = (B + groups - 1) / std::max<uint64_t>(groups, 1);
+        std::vector<cudaEvent_t> ev;
+        auto event = [&](cudaStream_t st) {
+            cudaEvent_t e;
+            ZK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            ev.push_back(e);
+            ZK_CUDA(cudaEventRecord(e, st));
+            return e;
+        };
+        try {
+            cudaStream_t cs = ctx.copy_stream;
+            ZK_CUDA(cudaStreamWaitEvent(cs, event(s), 0));  // after the allocations above
+            std::vector<cudaEvent_t> in_ready;
+            for (uint64_t b0 = 0; b0 < B; b0 += gsz) {
+                const uint64_t nb = std::min(gsz, B - b0);
+                if (!cfg.are_inputs_on_device)
+                    h2d(sin.as<uint64_t>() + b0 * n, (const uint64_t *)input + b0 * n, nb * n * sizeof(uint64_t), cs);
+                in_ready.push_back(event(cs));
+            }
+            size_t gi = 0;
+            for (uint64_t b0 = 0; b0 < B; b0 += gsz, gi++) {
+                const uint64_t nb = std::min(gsz, B - b0);
+                ZK_CUDA(cudaStreamWaitEvent(s, in_ready[gi], 0));
+                lde_device(ctx, d_out + b0 * N, d_in + b0 * n, lg_n, rb, nb, ntt_direction == inverse, cfg.with_coset,
+                           s);
+                if (!cfg.are_outputs_on_device) {
+                    ZK_CUDA(cudaStreamWaitEvent(cs, event(s), 0));
+                    d2h((uint64_t *)output + b0 * N, d_out + b0 * N, nb * N * sizeof(uint64_t), cs);
+                }
+            }
+            if (cfg.salt_size) {
+                salt_run(d_out + B * N, (uint64_t)cfg.salt_size * N, seed_now(), s);
+                if (!cfg.are_outputs_on_device) {
+                    ZK_CUDA(cudaStreamWaitEvent(cs, event(s), 0));
+                    d2h((uint64_t *)output + B * N, d_out + B * N, (uint64_t)cfg.salt_size * N * sizeof(uint64_t), cs);
+                }
+            }
+            ZK_CUDA(cudaStreamWaitEvent(s, event(cs), 0));  // the stream-ordered frees come after the copies
+            ZK_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            cudaStreamSynchronize(ctx.copy_stream);
+            cudaStreamSynchronize(s);
+            for (cudaEvent_t e : ev) cudaEventDestroy(e);
+            throw;
+        }
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
     });
 }
 

@@ -229,4 +229,25 @@ __device__ __forceinline__ uint64_t pr_reduce_split(uint64_t al, uint64_t ah, ui
     return ((uint64_t)r1 << 32) | r0;
 }
 
+// al + ah * 2^32 for al < 2^64 and ah < 2^64 - 2^33; partially reduced.
+__device__ __forceinline__ uint64_t pr_reduce_split_nc(uint64_t al, uint64_t ah) {
+    uint32_t r0 = (uint32_t)al, r1;
+    asm("{\n\t"
+        ".reg .u32 k, j;\n\t"
+        "add.cc.u32  %1, %3, %4;\n\t"   // r = al + lo32(ah) * 2^32
+        "addc.u32    k, %5, 0;\n\t"     // k = 2^64 carry + hi32(ah)
+        "add.cc.u32  %1, %1, k;\n\t"    // r += k * EPS = k * 2^32 - k
+        "addc.u32    j, 0, 0;\n\t"
+        "sub.cc.u32  %0, %0, k;\n\t"
+        "subc.cc.u32 %1, %1, 0;\n\t"
+        "subc.u32    j, j, 0;\n\t"      // j = 1 iff that overflowed 2^64
+        "neg.s32     j, j;\n\t"
+        "add.cc.u32  %0, %0, j;\n\t"
+        "addc.u32    %1, %1, 0;\n\t"
+        "}"
+        : "+r"(r0), "=r"(r1)
+        : "r"((uint32_t)al), "r"((uint32_t)(al >> 32)), "r"((uint32_t)ah), "r"((uint32_t)(ah >> 32)));
+    return ((uint64_t)r1 << 32) | r0;
+}
+
 }  // namespace zk

@@ -53,8 +53,27 @@ constexpr RcTable magic_adjusted(RcTable t) {
     return t;
 }
 
+// Poseidon: the next round's constant c goes into the FP64 accumulators
+// instead of the integer reduction.  With m = (c - kMagicAdj) mod p, the low
+// and high half-vector outputs of round rnd start from 2^52 + (m mod 2^32) and
+// 2^52 + floor(m / 2^32) (exact: both below 2^53), so that
+// bits(lo) + bits(hi) * 2^32 = MDS x + c (mod p).  Round 29 has no constant.
+struct MdsK {
+    double v[30][2][12];
+};
+constexpr MdsK make_mds_k(RcTable rc) {
+    MdsK t{};
+    for (int rnd = 0; rnd < 30; rnd++)
+        for (int r = 0; r < 12; r++) {
+            const uint64_t m = cx_sub_mod(rnd < 29 ? cx_canon(rc.v[12 * (rnd + 1) + r]) : 0, kMagicAdj);
+            t.v[rnd][0][r] = kMagic + (double)(m & 0xffffffffull);
+            t.v[rnd][1][r] = kMagic + (double)(m >> 32);
+        }
+    return t;
+}
+
 __constant__ uint64_t c_poseidon2_rc[360] = {ZK_POSEIDON2_RC_LIST};  // internal layer
-__constant__ RcTable c_poseidon_rcm = magic_adjusted(RcTable{{ZK_POSEIDON_RC_LIST}});
+__constant__ MdsK c_poseidon_mdsk = make_mds_k(RcTable{{ZK_POSEIDON_RC_LIST}});
 __constant__ RcTable c_poseidon2_rcm = magic_adjusted(RcTable{{ZK_POSEIDON2_RC_LIST}});
 __constant__ RcTable c_poseidon_rc = RcTable{{ZK_POSEIDON_RC_LIST}};  // round 0 is added before the first S-box
 __constant__ uint64_t c_poseidon2_diag[12] = {ZK_POSEIDON2_DIAG_LIST};
@@ -102,8 +121,8 @@ __host__ __device__ constexpr int mds_q2(int r, int k) {  // A - B, plus d on (0
 }
 #undef ZK_MDS_TABLES
 
-// One half-vector: a[i] = 2^52 + x[i] in, o[r] = 2^52 + (MDS x)[r] out.
-__device__ __forceinline__ void poseidon_mds_half(const double a[12], double o[12]) {
+// One half-vector: a[i] = 2^52 + x[i] in, o[r] = k[r] + (MDS x)[r] out.
+__device__ __forceinline__ void poseidon_mds_half(const double a[12], double o[12], const double *k) {
     double u[6], w[6], x6 = 0.0;
 #pragma unroll
     for (int i = 0; i < 6; i++) {
@@ -116,29 +135,30 @@ __device__ __forceinline__ void poseidon_mds_half(const double a[12], double o[1
     for (int r = 0; r < 6; r++) {
         double pa = (double)mds_p2(r, 0) * u[0], qa = (double)mds_q2(r, 0) * w[0];
 #pragma unroll
-        for (int k = 1; k < 6; k++) {
-            pa = fma((double)mds_p2(r, k), u[k], pa);
-            qa = fma((double)mds_q2(r, k), w[k], qa);
+        for (int c = 1; c < 6; c++) {
+            pa = fma((double)mds_p2(r, c), u[c], pa);
+            qa = fma((double)mds_q2(r, c), w[c], qa);
         }
         // The (0, 0) terms carry d (u + w) = 2 d x_lo[0] into lane 0; lane 6
         // must not get d (u - w) = 2 d x_hi[0], so it is taken out again.
         double d = pa - qa;
         if (r == 0) d = fma(-2.0 * (double)mds_diag0(), x6, d);
-        o[r] = fma(0.5, pa + qa, kMagic);
-        o[r + 6] = fma(0.5, d, kMagic);
+        o[r] = fma(0.5, pa + qa, k[r]);
+        o[r + 6] = fma(0.5, d, k[r + 6]);
     }
 }
 
-// s <- MDS s + c (c: the adjusted constants of the next round, or nullptr).
-__device__ __forceinline__ void poseidon_mds(uint64_t s[12], const uint64_t *cm) {
+// s <- MDS s + c, c being round rnd + 1's constants (none after round 29).
+__device__ __forceinline__ void poseidon_mds(uint64_t s[12], int rnd) {
     double a[12], lo[12], hi[12];
 #pragma unroll
     for (int i = 0; i < 12; i++) a[i] = magic_in((uint32_t)s[i]);
-    poseidon_mds_half(a, lo);
+    poseidon_mds_half(a, lo, c_poseidon_mdsk.v[rnd][0]);
 #pragma unroll
     for (int i = 0; i < 12; i++) a[i] = magic_in((uint32_t)(s[i] >> 32));
-    poseidon_mds_half(a, hi);
-    magic_combine(s, lo, hi, cm);
+    poseidon_mds_half(a, hi, c_poseidon_mdsk.v[rnd][1]);
+#pragma unroll
+    for (int r = 0; r < 12; r++) s[r] = pr_reduce_split_nc(magic_out(lo[r]), magic_out(hi[r]));
 }
 
 // x^7 on all 12 lanes, as three passes over 4 lanes with a rotation between
@@ -169,7 +189,7 @@ __device__ __forceinline__ void poseidon_permute(uint64_t s[12]) {
     for (int rnd = 0; rnd < 30; rnd++) {
         if (rnd < 4 || rnd >= 26) pow7_all(s);
         else s[0] = pr_pow7(s[0]);
-        poseidon_mds(s, rnd < 29 ? &c_poseidon_rcm.v[12 * (rnd + 1)] : nullptr);
+        poseidon_mds(s, rnd);
     }
 }
 

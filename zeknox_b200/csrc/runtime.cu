@@ -82,6 +82,7 @@ DeviceCtx &device_ctx(int dev) {
         // Blocking stream: work on it is ordered after the legacy default stream,
         // like zeknox's per-GPU "zero" stream (native/utils/gpu_t.cuh:246-252).
         ZK_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault));
+        ZK_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
         // Keep freed pool memory cached between calls.
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {

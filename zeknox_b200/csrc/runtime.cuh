@@ -79,6 +79,7 @@ constexpr int kLineLgMax = 12;  // longest in-shared-memory line: 4096 elements
 struct DeviceCtx {
     int dev = -1;
     cudaStream_t stream = nullptr;       // blocking stream (orders after the legacy stream)
+    cudaStream_t copy_stream = nullptr;  // host<->device copies overlapped with `stream`
     uint64_t *line_roots[2] = {nullptr, nullptr};  // [dir] omega_4096^j, j < 4096
     PowTable roots[2][kMaxLg + 1];       // [dir][lg]: omega_{2^lg} powers
     PowTable coset;                      // coset_gen powers
