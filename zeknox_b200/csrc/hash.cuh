@@ -72,12 +72,41 @@ constexpr MdsK make_mds_k(RcTable rc) {
     return t;
 }
 
-__constant__ uint64_t c_poseidon2_rc[360] = {ZK_POSEIDON2_RC_LIST};  // internal layer
-__constant__ MdsK c_poseidon_mdsk = make_mds_k(RcTable{{ZK_POSEIDON_RC_LIST}});
-__constant__ RcTable c_poseidon2_rcm = magic_adjusted(RcTable{{ZK_POSEIDON2_RC_LIST}});
-__constant__ RcTable c_poseidon_rc = RcTable{{ZK_POSEIDON_RC_LIST}};  // round 0 is added before the first S-box
-__constant__ uint64_t c_poseidon2_diag[12] = {ZK_POSEIDON2_DIAG_LIST};
+// The round tables of one hasher.  Permutations read them from the
+// __constant__ bank (kernels with many resident warps keep it hot) or from a
+// block's shared-memory copy of the __device__ twin (latency-bound kernels
+// with a few warps, which would otherwise wait on a constant-cache miss in
+// every round).
+struct PoseidonTab {
+    MdsK mdsk;         // next-round constants inside the MDS accumulators
+    uint64_t rc0[12];  // round 0, added before the first S-box
+};
+struct Poseidon2Tab {
+    RcTable rcm;        // external rounds: adjusted for the magic offsets
+    RcTable rc;         // internal rounds (lane 0) and the first external round after them
+    uint64_t diag[12];  // internal-layer diagonal
+};
+struct KeccakTab {};
+constexpr PoseidonTab make_poseidon_tab(RcTable rc) {
+    PoseidonTab t{};
+    t.mdsk = make_mds_k(rc);
+    for (int i = 0; i < 12; i++) t.rc0[i] = cx_canon(rc.v[i]);
+    return t;
+}
+constexpr Poseidon2Tab make_poseidon2_tab(RcTable rc) {
+    Poseidon2Tab t{};
+    t.rcm = magic_adjusted(rc);
+    t.rc = rc;
+    constexpr uint64_t d[12] = {ZK_POSEIDON2_DIAG_LIST};
+    for (int i = 0; i < 12; i++) t.diag[i] = d[i];
+    return t;
+}
+__constant__ PoseidonTab c_poseidon = make_poseidon_tab(RcTable{{ZK_POSEIDON_RC_LIST}});
+__constant__ Poseidon2Tab c_poseidon2 = make_poseidon2_tab(RcTable{{ZK_POSEIDON2_RC_LIST}});
+__device__ PoseidonTab g_poseidon = make_poseidon_tab(RcTable{{ZK_POSEIDON_RC_LIST}});
+__device__ Poseidon2Tab g_poseidon2 = make_poseidon2_tab(RcTable{{ZK_POSEIDON2_RC_LIST}});
 __constant__ uint64_t c_keccak_rc[24] = {ZK_KECCAK_RC_LIST};
+__constant__ KeccakTab c_keccak_tab;
 
 __device__ __forceinline__ double magic_in(uint32_t x) { return __hiloint2double(0x43300000, (int)x); }
 __device__ __forceinline__ uint64_t magic_out(double v) { return (uint64_t)__double_as_longlong(v); }
@@ -133,12 +162,16 @@ __device__ __forceinline__ void poseidon_mds_half(const double a[12], double o[1
     }
 #pragma unroll
     for (int r = 0; r < 6; r++) {
-        double pa = (double)mds_p2(r, 0) * u[0], qa = (double)mds_q2(r, 0) * w[0];
+        // Lanes 0 and 6 (u[0], w[0]) last: in a partial round only lane 0 has
+        // just left the S-box, so the other terms need not wait for it.
+        double pa = (double)mds_p2(r, 1) * u[1], qa = (double)mds_q2(r, 1) * w[1];
 #pragma unroll
-        for (int c = 1; c < 6; c++) {
+        for (int c = 2; c < 6; c++) {
             pa = fma((double)mds_p2(r, c), u[c], pa);
             qa = fma((double)mds_q2(r, c), w[c], qa);
         }
+        pa = fma((double)mds_p2(r, 0), u[0], pa);
+        qa = fma((double)mds_q2(r, 0), w[0], qa);
         // The (0, 0) terms carry d (u + w) = 2 d x_lo[0] into lane 0; lane 6
         // must not get d (u - w) = 2 d x_hi[0], so it is taken out again.
         double d = pa - qa;
@@ -149,32 +182,40 @@ __device__ __forceinline__ void poseidon_mds_half(const double a[12], double o[1
 }
 
 // s <- MDS s + c, c being round rnd + 1's constants (none after round 29).
-__device__ __forceinline__ void poseidon_mds(uint64_t s[12], int rnd) {
+__device__ __forceinline__ void poseidon_mds(uint64_t s[12], int rnd, const PoseidonTab &tab) {
     double a[12], lo[12], hi[12];
 #pragma unroll
     for (int i = 0; i < 12; i++) a[i] = magic_in((uint32_t)s[i]);
-    poseidon_mds_half(a, lo, c_poseidon_mdsk.v[rnd][0]);
+    poseidon_mds_half(a, lo, tab.mdsk.v[rnd][0]);
 #pragma unroll
     for (int i = 0; i < 12; i++) a[i] = magic_in((uint32_t)(s[i] >> 32));
-    poseidon_mds_half(a, hi, c_poseidon_mdsk.v[rnd][1]);
+    poseidon_mds_half(a, hi, tab.mdsk.v[rnd][1]);
 #pragma unroll
     for (int r = 0; r < 12; r++) s[r] = pr_reduce_split_nc(magic_out(lo[r]), magic_out(hi[r]));
 }
 
-// x^7 on all 12 lanes, as three passes over 4 lanes with a rotation between
-// them (keeps the loop body, and so the instruction footprint, small).
+// x^7 on all 12 lanes.  W = 4: three passes over 4 lanes with a rotation
+// between them (a small loop body, and so a small instruction footprint, for
+// kernels with many resident warps).  W = 12: all lanes at once (more
+// independent work in flight, for kernels whose few warps wait on latency).
+template <int W = 4>
 __device__ __forceinline__ void pow7_all(uint64_t s[12]) {
+    if constexpr (W == 12) {
+#pragma unroll
+        for (int i = 0; i < 12; i++) s[i] = pr_pow7(s[i]);
+    } else {
 #pragma unroll 1
-    for (int q = 0; q < 3; q++) {
+        for (int q = 0; q < 3; q++) {
 #pragma unroll
-        for (int i = 0; i < 4; i++) s[i] = pr_pow7(s[i]);
-        const uint64_t t0 = s[0], t1 = s[1], t2 = s[2], t3 = s[3];
+            for (int i = 0; i < 4; i++) s[i] = pr_pow7(s[i]);
+            const uint64_t t0 = s[0], t1 = s[1], t2 = s[2], t3 = s[3];
 #pragma unroll
-        for (int i = 0; i < 8; i++) s[i] = s[i + 4];
-        s[8] = t0;
-        s[9] = t1;
-        s[10] = t2;
-        s[11] = t3;
+            for (int i = 0; i < 8; i++) s[i] = s[i + 4];
+            s[8] = t0;
+            s[9] = t1;
+            s[10] = t2;
+            s[11] = t3;
+        }
     }
 }
 
@@ -182,14 +223,15 @@ __device__ __forceinline__ void pow7_all(uint64_t s[12]) {
 // Round r adds its 12 constants, applies x^7 (all lanes in rounds 0-3 and
 // 26-29, lane 0 otherwise) and the MDS layer; each round's constants are
 // added inside the previous round's MDS reduction.
-__device__ __forceinline__ void poseidon_permute(uint64_t s[12]) {
+template <int W = 4>
+__device__ __forceinline__ void poseidon_permute(uint64_t s[12], const PoseidonTab &tab = c_poseidon) {
 #pragma unroll
-    for (int i = 0; i < 12; i++) s[i] = pr_add_c(s[i], c_poseidon_rc.v[i]);
+    for (int i = 0; i < 12; i++) s[i] = pr_add_c(s[i], tab.rc0[i]);
 #pragma unroll 1
     for (int rnd = 0; rnd < 30; rnd++) {
-        if (rnd < 4 || rnd >= 26) pow7_all(s);
+        if (rnd < 4 || rnd >= 26) pow7_all<W>(s);
         else s[0] = pr_pow7(s[0]);
-        poseidon_mds(s, rnd);
+        poseidon_mds(s, rnd, tab);
     }
 }
 
@@ -235,7 +277,7 @@ __device__ __forceinline__ void poseidon2_external(uint64_t s[12], const uint64_
 
 // x_i <- x_i * D_i + sum_j x_j (+ next round's constants): poseidon2.cu:131-146.
 // The sum of the 12 lanes is kept exact in 96 bits (carry chain).
-__device__ __forceinline__ void poseidon2_internal(uint64_t s[12], const uint64_t *c) {
+__device__ __forceinline__ void poseidon2_internal(uint64_t s[12], const uint64_t *c, const uint64_t *diag) {
     uint32_t s0 = (uint32_t)s[0], s1 = (uint32_t)(s[0] >> 32), s2 = 0;
 #pragma unroll
     for (int i = 1; i < 12; i++) {
@@ -253,27 +295,28 @@ __device__ __forceinline__ void poseidon2_internal(uint64_t s[12], const uint64_
             "addc.u32 %2, %5, 0;"
             : "=r"(c0), "=r"(c1), "=r"(c2)
             : "r"(s0), "r"(s1), "r"(s2), "r"((uint32_t)c[i]), "r"((uint32_t)(c[i] >> 32)));
-        s[i] = pr_mul_add(s[i], c_poseidon2_diag[i], ((uint64_t)c1 << 32) | c0, c2);
+        s[i] = pr_mul_add(s[i], diag[i], ((uint64_t)c1 << 32) | c0, c2);
     }
 }
 
-__device__ __forceinline__ void poseidon2_permute(uint64_t s[12]) {
-    poseidon2_external(s, &c_poseidon2_rcm.v[0]);
+template <int W = 4>
+__device__ __forceinline__ void poseidon2_permute(uint64_t s[12], const Poseidon2Tab &tab = c_poseidon2) {
+    poseidon2_external(s, &tab.rcm.v[0]);
 #pragma unroll 1
     for (int rnd = 0; rnd < 4; rnd++) {
-        pow7_all(s);
-        poseidon2_external(s, &c_poseidon2_rcm.v[12 * (rnd + 1)]);
+        pow7_all<W>(s);
+        poseidon2_external(s, &tab.rcm.v[12 * (rnd + 1)]);
     }
     // internal rounds: only lane 0 of their constants is non-zero
 #pragma unroll 1
     for (int rnd = 4; rnd < 26; rnd++) {
         s[0] = pr_pow7(s[0]);
-        poseidon2_internal(s, &c_poseidon2_rc[12 * (rnd + 1)]);
+        poseidon2_internal(s, &tab.rc.v[12 * (rnd + 1)], tab.diag);
     }
 #pragma unroll 1
     for (int rnd = 26; rnd < 30; rnd++) {
-        pow7_all(s);
-        poseidon2_external(s, rnd < 29 ? &c_poseidon2_rcm.v[12 * (rnd + 1)] : nullptr);
+        pow7_all<W>(s);
+        poseidon2_external(s, rnd < 29 ? &tab.rcm.v[12 * (rnd + 1)] : nullptr);
     }
 }
 
@@ -374,7 +417,38 @@ __device__ __forceinline__ void hash_one(const uint64_t *__restrict__ in, uint32
 }
 
 template <int H>
-__device__ __forceinline__ void hash_two(const uint64_t *l, const uint64_t *r, uint64_t *out) {
+struct TabOf;
+template <>
+struct TabOf<kPoseidon> {
+    using type = PoseidonTab;
+};
+template <>
+struct TabOf<kPoseidon2> {
+    using type = Poseidon2Tab;
+};
+template <>
+struct TabOf<kKeccak> {
+    using type = KeccakTab;
+};
+template <int H>
+__device__ __forceinline__ const typename TabOf<H>::type &const_tab() {
+    if constexpr (H == kPoseidon) return c_poseidon;
+    else if constexpr (H == kPoseidon2) return c_poseidon2;
+    else return c_keccak_tab;
+}
+
+// The __device__ twin of a hasher's tables (source of shared-memory copies).
+template <int H>
+__device__ __forceinline__ const typename TabOf<H>::type *global_tab() {
+    if constexpr (H == kPoseidon) return &g_poseidon;
+    else if constexpr (H == kPoseidon2) return &g_poseidon2;
+    else return nullptr;
+}
+
+// H(l || r) of two digests; W and tab choose the S-box width and the table copy.
+template <int H, int W = 4>
+__device__ __forceinline__ void hash_two(const uint64_t *l, const uint64_t *r, uint64_t *out,
+                                         const typename TabOf<H>::type &tab = const_tab<H>()) {
     if constexpr (H == kKeccak) {
         // keccak256(left[0..25) || right[0..25)): 50 bytes in one block
         uint64_t a[25];
@@ -402,8 +476,8 @@ __device__ __forceinline__ void hash_two(const uint64_t *l, const uint64_t *r, u
             s[4 + i] = gl_canon(r[i]);
             s[8 + i] = 0;
         }
-        if constexpr (H == kPoseidon) poseidon_permute(s);
-        else poseidon2_permute(s);
+        if constexpr (H == kPoseidon) poseidon_permute<W>(s, tab);
+        else poseidon2_permute<W>(s, tab);
         out[0] = gl_canon(s[0]);
         out[1] = gl_canon(s[1]);
         out[2] = gl_canon(s[2]);

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(kLeafThreads) merkle_leaves(const uint64_t *__
 
 // One level of width w = 2^lg_w nodes per subtree (at offsets w - 2 .. 2w - 3
 // of each subtree's block): node i <- H(node 2(i+1), node 2(i+1)+1).
-template <int H>
+template <int H, int W>
 __global__ void __launch_bounds__(kLeafThreads) merkle_level(uint64_t *__restrict__ digests, uint32_t lg_w,
                                                              uint64_t n_caps, uint64_t ds) {
     const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -54,15 +54,38 @@ __global__ void __launch_bounds__(kLeafThreads) merkle_level(uint64_t *__restric
     if (tid >= (n_caps << lg_w)) return;
     const uint64_t s = tid >> lg_w, i = (w - 2) + (tid & (w - 1));
     uint64_t *base = digests + 4 * s * ds;
-    hash_two<H>(base + 4 * (2 * i + 2), base + 4 * (2 * i + 3), base + 4 * i);
+    hash_two<H, W>(base + 4 * (2 * i + 2), base + 4 * (2 * i + 3), base + 4 * i);
 }
 
+// One block per subtree: the levels of width w_top, w_top/2, ..., 1 (the cap),
+// one node per thread, __syncthreads between levels.  These levels are few
+// nodes each, so every one costs about one permutation's latency: the block
+// copies its hasher's round tables into shared memory first and uses the
+// 12-lanes-at-once S-box.
 template <int H>
-__global__ void merkle_caps(uint64_t *__restrict__ cap, const uint64_t *__restrict__ digests, uint64_t n_caps,
-                            uint64_t ds) {
-    const uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (s >= n_caps) return;
-    hash_two<H>(digests + 4 * s * ds, digests + 4 * (s * ds + 1), cap + 4 * s);
+__global__ void __launch_bounds__(256) merkle_top(uint64_t *__restrict__ digests, uint64_t *__restrict__ cap,
+                                                   uint64_t ds, uint32_t w_top) {
+    using Tab = typename TabOf<H>::type;
+    __shared__ __align__(16) unsigned char tab_raw[sizeof(Tab)];
+    Tab &tab = *reinterpret_cast<Tab *>(tab_raw);
+    if constexpr (sizeof(Tab) >= 8) {
+        const uint64_t *g = reinterpret_cast<const uint64_t *>(global_tab<H>());
+        uint64_t *d = reinterpret_cast<uint64_t *>(tab_raw);
+        for (uint32_t k = threadIdx.x; k < sizeof(Tab) / 8; k += blockDim.x) d[k] = g[k];
+    }
+    __syncthreads();
+    const uint64_t sub = blockIdx.x;
+    uint64_t *base = digests + 4 * sub * ds;
+    for (uint32_t w = w_top; w >= 1; w >>= 1) {
+        const uint32_t i = threadIdx.x;
+        if (i < w) {
+            const uint64_t *c = base + 4 * (2 * w - 2 + 2 * i);  // children 2i, 2i+1 of the level of width 2w
+            uint64_t *o = w >= 2 ? base + 4 * (w - 2 + i) : cap + 4 * sub;
+            if constexpr (sizeof(Tab) >= 8) hash_two<H, 12>(c, c + 4, o, tab);
+            else hash_two<H, 12>(c, c + 4, o);
+        }
+        __syncthreads();
+    }
 }
 
 inline unsigned blocks_for(uint64_t n, unsigned tpb) {
@@ -97,12 +120,20 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
     merkle_leaves<H><<<blocks_for(j.n_leaves, kLeafThreads), kLeafThreads, 0, st>>>(j.leaves, j.n_leaves, w, j.digests,
                                                                                      map);
     ZK_CHECK_LAUNCH();
-    for (uint32_t lg_w = map.lg_ls - 1; lg_w >= 1; lg_w--) {
-        merkle_level<H><<<blocks_for(j.n_caps << lg_w, kLeafThreads), kLeafThreads, 0, st>>>(j.digests, lg_w,
-                                                                                              j.n_caps, ds);
+    // Wide levels: one launch each, one node per thread.  The narrow top
+    // (fewer than kNarrow nodes in all, at most 256 per subtree) goes to
+    // merkle_top in one launch.
+    constexpr uint64_t kNarrow = 1 << 14;
+    uint32_t lg_top = 0;
+    while (lg_top + 1 < map.lg_ls && lg_top < 8 && (j.n_caps << (lg_top + 1)) < kNarrow) lg_top++;
+    for (uint32_t lg_w = map.lg_ls - 1; lg_w > lg_top; lg_w--) {
+        merkle_level<H, 4><<<blocks_for(j.n_caps << lg_w, kLeafThreads), kLeafThreads, 0, st>>>(j.digests, lg_w,
+                                                                                                 j.n_caps, ds);
         ZK_CHECK_LAUNCH();
     }
-    merkle_caps<H><<<blocks_for(j.n_caps, 64), 64, 0, st>>>(j.cap, j.digests, j.n_caps, ds);
+    require(j.n_caps < (1ull << 31), "too many subtrees");
+    const uint32_t w_top = 1u << lg_top;
+    merkle_top<H><<<(unsigned)j.n_caps, std::max<uint32_t>(32, w_top), 0, st>>>(j.digests, j.cap, ds, w_top);
     ZK_CHECK_LAUNCH();
 }
 
