@@ -356,7 +356,7 @@ __device__ __forceinline__ void keccak_f1600(uint64_t a[25]) {
 enum : int { kPoseidon = 0, kKeccak = 1, kPoseidon2 = 3 };
 
 // Leaf elements are reduced mod p when read (a no-op for canonical inputs).
-template <int H>
+template <int H, int W = 4>
 __device__ __forceinline__ void hash_one(const uint64_t *__restrict__ in, uint32_t n, uint64_t *__restrict__ out) {
     if constexpr (H == kKeccak) {
         if (n < 4) {  // copy n words, leave the rest of the digest as it was
@@ -406,8 +406,8 @@ __device__ __forceinline__ void hash_one(const uint64_t *__restrict__ in, uint32
                 for (int j = 0; j < 8; j++)
                     if ((uint32_t)j < len) s[j] = gl_canon(in[idx + j]);
             }
-            if constexpr (H == kPoseidon) poseidon_permute(s);
-            else poseidon2_permute(s);
+            if constexpr (H == kPoseidon) poseidon_permute<W>(s);
+            else poseidon2_permute<W>(s);
         }
         out[0] = gl_canon(s[0]);
         out[1] = gl_canon(s[1]);
