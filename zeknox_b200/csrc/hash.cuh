@@ -485,4 +485,119 @@ __device__ __forceinline__ void hash_two(const uint64_t *l, const uint64_t *r, u
     }
 }
 
+// ------------------------------------------- Poseidon on six threads
+// For the latency-bound parts (narrow tree levels, small trees) one
+// permutation is spread over a group of six consecutive lanes of a warp
+// (five groups per warp; lanes 30 and 31 compute on dummy data).  Group
+// thread t owns lanes t and t + 6.  Each round: the S-box on the owned lanes
+// (lane 0 only, on thread 0, in partial rounds), an all-gather of the 12
+// lanes by shuffles (every shuffle reads one thread of the group, so all
+// threads get the lanes in natural order), then thread t computes the MDS
+// row pair (t, t + 6) of the split above: rows of A + B and A - B held in
+// registers.  About a third of the single-thread path's instructions per
+// thread, so about a third of its latency.
+struct HexGroup {
+    uint32_t t;     // thread within the group, 0..5 (lanes 30, 31: 0..1 of a dummy group)
+    uint32_t base;  // warp lane of the group's thread 0
+    double p2[6], q2[6];  // row t of A + B and A - B (with the diagonal term on row 0)
+    double fix6;          // -2 d on thread 0 (lane 6 must not get the diagonal), else 0
+    __device__ __forceinline__ HexGroup() {
+        const uint32_t lane = threadIdx.x & 31;
+        const uint32_t g = lane < 30 ? lane / 6 : 0;
+        t = lane < 30 ? lane % 6 : lane - 30;
+        base = 6 * g;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            p2[k] = (double)mds_p2((int)t, k);
+            q2[k] = (double)mds_q2((int)t, k);
+        }
+        fix6 = t == 0 ? -2.0 * (double)mds_diag0() : 0.0;
+    }
+    // true for the lanes whose group is a real one (not lanes 30, 31)
+    __device__ __forceinline__ bool real() const { return (threadIdx.x & 31) < 30; }
+    __device__ __forceinline__ uint32_t group_in_warp() const { return base / 6; }
+};
+
+__device__ __forceinline__ uint64_t shfl64(uint64_t v, uint32_t src) {
+    return (uint64_t)__shfl_sync(0xffffffffu, (long long)v, (int)src);
+}
+
+// o0, o1: lanes t and t + 6 of the state (partially reduced, in and out).
+// Every lane of the warp must call this (shuffles over the full warp).
+__device__ __forceinline__ void poseidon_permute_hex(uint64_t &o0, uint64_t &o1, const HexGroup &g,
+                                                     const PoseidonTab &tab) {
+    o0 = pr_add_c(o0, tab.rc0[g.t]);
+    o1 = pr_add_c(o1, tab.rc0[g.t + 6]);
+#pragma unroll 1
+    for (int rnd = 0; rnd < 30; rnd++) {
+        if (rnd < 4 || rnd >= 26) {
+            o0 = pr_pow7(o0);
+            o1 = pr_pow7(o1);
+        } else {
+            const uint64_t y = pr_pow7(o0);
+            if (g.t == 0) o0 = y;
+        }
+        uint64_t x[12];
+#pragma unroll
+        for (int i = 0; i < 12; i++) x[i] = shfl64(i < 6 ? o0 : o1, g.base + (i % 6));
+        double first[2], second[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            double u[6], w[6], x6 = 0.0;
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+                const double a = magic_in(h ? (uint32_t)(x[i] >> 32) : (uint32_t)x[i]);
+                const double b = magic_in(h ? (uint32_t)(x[i + 6] >> 32) : (uint32_t)x[i + 6]);
+                const double tb = b - kMagic;
+                if (i == 0) x6 = tb;
+                w[i] = a - b;
+                u[i] = fma(2.0, tb, w[i]);
+            }
+            double pa = g.p2[0] * u[0], qa = g.q2[0] * w[0];
+#pragma unroll
+            for (int k = 1; k < 6; k++) {
+                pa = fma(g.p2[k], u[k], pa);
+                qa = fma(g.q2[k], w[k], qa);
+            }
+            const double d = fma(g.fix6, x6, pa - qa);
+            first[h] = fma(0.5, pa + qa, tab.mdsk.v[rnd][h][g.t]);
+            second[h] = fma(0.5, d, tab.mdsk.v[rnd][h][g.t + 6]);
+        }
+        o0 = pr_reduce_split_nc(magic_out(first[0]), magic_out(first[1]));
+        o1 = pr_reduce_split_nc(magic_out(second[0]), magic_out(second[1]));
+    }
+}
+
+// H(l || r) on a group: every lane calls; `active` groups load and store.
+__device__ __forceinline__ void poseidon_hash_two_hex(const uint64_t *l, const uint64_t *r, uint64_t *out,
+                                                      bool active, const HexGroup &g, const PoseidonTab &tab) {
+    uint64_t o0 = 0, o1 = 0;
+    if (active) {
+        o0 = gl_canon(g.t < 4 ? l[g.t] : r[g.t - 4]);
+        if (g.t < 2) o1 = gl_canon(r[g.t + 2]);
+    }
+    poseidon_permute_hex(o0, o1, g, tab);
+    if (active && g.t < 4) out[g.t] = gl_canon(o0);
+}
+
+// Sponge of n words (zeknox's hash_or_noop: n <= 4 copies and zero-pads).
+// n must be the same for all groups of a warp.
+__device__ __forceinline__ void poseidon_hash_one_hex(const uint64_t *in, uint32_t n, uint64_t *out, bool active,
+                                                      const HexGroup &g, const PoseidonTab &tab) {
+    if (n <= 4) {
+        if (active && g.t < 4) out[g.t] = g.t < n ? in[g.t] : 0ull;
+        return;
+    }
+    uint64_t o0 = 0, o1 = 0;
+    for (uint32_t idx = 0; idx < n; idx += 8) {
+        const uint32_t len = n - idx < 8 ? n - idx : 8;
+        if (active) {
+            if (g.t < len) o0 = gl_canon(in[idx + g.t]);
+            if (g.t + 6 < len) o1 = gl_canon(in[idx + g.t + 6]);
+        }
+        poseidon_permute_hex(o0, o1, g, tab);
+    }
+    if (active && g.t < 4) out[g.t] = gl_canon(o0);
+}
+
 }  // namespace zk

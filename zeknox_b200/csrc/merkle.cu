@@ -90,6 +90,77 @@ __global__ void __launch_bounds__(256) merkle_top(uint64_t *__restrict__ digests
     }
 }
 
+// Copies a hasher's round tables into shared memory (all threads of the block).
+template <int H>
+__device__ __forceinline__ void load_tab(typename TabOf<H>::type &dst) {
+    const uint64_t *g = reinterpret_cast<const uint64_t *>(global_tab<H>());
+    uint64_t *d = reinterpret_cast<uint64_t *>(&dst);
+    for (uint32_t k = threadIdx.x; k < sizeof(dst) / 8; k += blockDim.x) d[k] = g[k];
+    __syncthreads();
+}
+
+// Poseidon on six threads per hash (HexGroup): five hashes per warp.  For the
+// latency-bound cases: few leaves, narrow levels, the top of the tree.
+constexpr int kHexThreads = 128;  // 4 warps = 20 hashes per block
+constexpr uint64_t kHexPerBlock = 20;
+
+__global__ void __launch_bounds__(kHexThreads) merkle_leaves_hex(const uint64_t *__restrict__ leaves,
+                                                                 uint64_t n_leaves, uint32_t leaf_size,
+                                                                 uint64_t *__restrict__ out, LeafMap map) {
+    __shared__ PoseidonTab tab;
+    load_tab<kPoseidon>(tab);
+    const HexGroup g;
+    const uint64_t first = ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5) * 5;
+    if (first >= n_leaves) return;  // whole warp
+    const uint64_t i = first + g.group_in_warp();
+    const bool active = g.real() && i < n_leaves;
+    const uint64_t ii = active ? i : 0;
+    poseidon_hash_one_hex(leaves + ii * leaf_size, leaf_size, out + 4 * map.slot(ii), active, g, tab);
+}
+
+__global__ void __launch_bounds__(kHexThreads) merkle_level_hex(uint64_t *__restrict__ digests, uint32_t lg_w,
+                                                                uint64_t n_caps, uint64_t ds) {
+    __shared__ PoseidonTab tab;
+    load_tab<kPoseidon>(tab);
+    const HexGroup g;
+    const uint64_t w = 1ull << lg_w;
+    const uint64_t first = ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5) * 5;
+    if (first >= (n_caps << lg_w)) return;  // whole warp
+    const uint64_t tid = first + g.group_in_warp();
+    const bool active = g.real() && tid < (n_caps << lg_w);
+    const uint64_t tt = active ? tid : 0;
+    const uint64_t sub = tt >> lg_w, i = (w - 2) + (tt & (w - 1));
+    uint64_t *base = digests + 4 * sub * ds;
+    poseidon_hash_two_hex(base + 4 * (2 * i + 2), base + 4 * (2 * i + 3), base + 4 * i, active, g, tab);
+}
+
+// One block per subtree: levels of width w_top (<= 32) .. 1, then the cap.
+__global__ void __launch_bounds__(224) merkle_top_hex(uint64_t *__restrict__ digests, uint64_t *__restrict__ cap,
+                                                       uint64_t ds, uint32_t w_top) {
+    __shared__ PoseidonTab tab;
+    load_tab<kPoseidon>(tab);
+    const HexGroup g;
+    const uint64_t sub = blockIdx.x;
+    uint64_t *base = digests + 4 * sub * ds;
+    const uint32_t node = (threadIdx.x >> 5) * 5 + g.group_in_warp();
+    for (uint32_t w = w_top; w >= 1; w >>= 1) {
+        if ((threadIdx.x >> 5) * 5 < w) {  // warps with at least one node of this level
+            const bool active = g.real() && node < w;
+            const uint32_t i = active ? node : 0;
+            const uint64_t *c = base + 4 * (2 * w - 2 + 2 * i);  // children 2i, 2i+1 of the level of width 2w
+            uint64_t *o = w >= 2 ? base + 4 * (w - 2 + i) : cap + 4 * sub;
+            poseidon_hash_two_hex(c, c + 4, o, active, g, tab);
+        }
+        __syncthreads();
+    }
+}
+
+inline unsigned hex_blocks(uint64_t hashes) {
+    const uint64_t b = (hashes + kHexPerBlock - 1) / kHexPerBlock;
+    require(b < (1ull << 31), "Merkle launch too large");
+    return (unsigned)(b ? b : 1);
+}
+
 inline unsigned blocks_for(uint64_t n, unsigned tpb) {
     const uint64_t b = (n + tpb - 1) / tpb;
     require(b < (1ull << 31), "Merkle launch too large");
@@ -119,6 +190,38 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
     map.direct = (ls == 2);
     map.lg_ls = (uint32_t)__builtin_ctzll(ls);
     map.ds = ds;
+    if constexpr (H == kPoseidon) {
+        // Latency-bound parts on six threads per hash: trees of at most
+        // kHexLeaves leaves, levels of fewer than kHexNodes nodes, and the
+        // top (<= 32 nodes per subtree, so that one SM per subtree stays
+        // latency- rather than issue-bound) in one launch.  Measured per
+        // level: 16384 nodes 46 us six-threaded vs 40 us one-threaded (issue
+        // bound: six threads do twice the instructions of one); 4096 nodes
+        // 20 us vs 40 us.
+        constexpr uint64_t kHexLeaves = 1 << 15, kHexNodes = 1 << 14;
+        if (j.n_leaves <= kHexLeaves)
+            merkle_leaves_hex<<<hex_blocks(j.n_leaves), kHexThreads, 0, st>>>(j.leaves, j.n_leaves, w, j.digests, map);
+        else
+            merkle_leaves<H><<<blocks_for(j.n_leaves, kLeafThreads), kLeafThreads, 0, st>>>(j.leaves, j.n_leaves, w,
+                                                                                             j.digests, map);
+        ZK_CHECK_LAUNCH();
+        uint32_t lg_top = 0;
+        while (lg_top + 1 < map.lg_ls && lg_top < 5 && (j.n_caps << (lg_top + 1)) < kHexNodes) lg_top++;
+        for (uint32_t lg_w = map.lg_ls - 1; lg_w > lg_top; lg_w--) {
+            const uint64_t nodes = j.n_caps << lg_w;
+            if (nodes >= kHexNodes)
+                merkle_level<H, 4><<<blocks_for(nodes, kLeafThreads), kLeafThreads, 0, st>>>(j.digests, lg_w, j.n_caps,
+                                                                                             ds);
+            else
+                merkle_level_hex<<<hex_blocks(nodes), kHexThreads, 0, st>>>(j.digests, lg_w, j.n_caps, ds);
+            ZK_CHECK_LAUNCH();
+        }
+        require(j.n_caps < (1ull << 31), "too many subtrees");
+        const uint32_t w_top = 1u << lg_top;
+        merkle_top_hex<<<(unsigned)j.n_caps, 32 * ((w_top + 4) / 5), 0, st>>>(j.digests, j.cap, ds, w_top);
+        ZK_CHECK_LAUNCH();
+        return;
+    }
     merkle_leaves<H><<<blocks_for(j.n_leaves, kLeafThreads), kLeafThreads, 0, st>>>(j.leaves, j.n_leaves, w, j.digests,
                                                                                      map);
     ZK_CHECK_LAUNCH();
