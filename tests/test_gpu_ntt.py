@@ -164,7 +164,8 @@ def test_init_coset_other_generator(zk, oracle):
         zk.init_coset(0, 20, 7)
 
 
-@pytest.mark.parametrize("lg,batches", [(0, 1), (1, 3), (5, 7), (10, 135), (13, 16), (18, 135), (6, 1000)])
+@pytest.mark.parametrize("lg,batches", [(0, 1), (1, 3), (5, 7), (10, 135), (13, 16), (18, 135), (6, 1000), (4, 200),
+                                        (7, 193)])
 def test_transpose_rev(zk, oracle, lg, batches):
     x = oracle.field_elems(9 + lg, batches << lg)
     out = np.zeros_like(x)

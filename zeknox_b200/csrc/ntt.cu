@@ -309,27 +309,45 @@ __global__ void __launch_bounds__(kNttThreads) ntt_last_pass_leaves(PassArgs a) 
 }
 
 
-// out[rev(k) * B + b] = in[b * N + k]: 16 rows x 64 columns per block, through
-// shared memory so both sides are coalesced (zeknox kernels.cu:94-135).
-constexpr int kTrRows = 16, kTrCols = 64;
+// out[rev(k) * B + b] = in[b * N + k] (zeknox kernels.cu:94-135).  A block
+// takes kTrK consecutive k of a chunk of up to kTrMaxPolys polynomials
+// (reads: kTrK contiguous words per polynomial) and writes each of the kTrK
+// output rows as one contiguous run of the chunk's words, so a chunk holding
+// every polynomial writes whole leaf rows.  The shared tile is [k][poly] with
+// an odd row pitch (no bank conflicts on either side).
+constexpr int kTrK = 32;
+constexpr uint32_t kTrMaxPolys = 192;
 __global__ void __launch_bounds__(256) transpose_rev_kernel(uint64_t *__restrict__ out, const uint64_t *__restrict__ in,
-                                                            uint32_t lg_n, uint32_t batches) {
-    __shared__ uint64_t tile[kTrCols * (kTrRows + 1)];
+                                                            uint32_t lg_n, uint32_t batches, uint32_t chunk) {
+    extern __shared__ uint64_t tile[];
     const uint64_t N = 1ull << lg_n;
-    const uint64_t k0 = (uint64_t)blockIdx.x * kTrCols;
-    const uint32_t b0 = blockIdx.y * kTrRows;
-    for (uint32_t idx = threadIdx.x; idx < kTrRows * kTrCols; idx += blockDim.x) {
-        const uint32_t bl = idx / kTrCols, kl = idx % kTrCols;
-        if (b0 + bl < batches && k0 + kl < N) tile[kl * (kTrRows + 1) + bl] = in[(uint64_t)(b0 + bl) * N + k0 + kl];
+    const uint32_t K = N < (uint64_t)kTrK ? (uint32_t)N : kTrK;
+    const uint64_t k0 = (uint64_t)blockIdx.x * K;
+    const uint32_t b0 = blockIdx.y * chunk;
+    const uint32_t nb = min(chunk, batches - b0);
+    const uint32_t pitch = nb | 1;
+    if (K == kTrK) {  // 16-byte loads of two consecutive k (k0 is a multiple of 32)
+        constexpr uint32_t H = kTrK / 2;
+#pragma unroll 4
+        for (uint32_t idx = threadIdx.x; idx < nb * H; idx += blockDim.x) {
+            const uint32_t bl = idx / H, kl = 2 * (idx % H);
+            const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(in + (uint64_t)(b0 + bl) * N + k0 + kl);
+            tile[kl * pitch + bl] = v.x;
+            tile[(kl + 1) * pitch + bl] = v.y;
+        }
+    } else {
+        for (uint32_t idx = threadIdx.x; idx < nb * K; idx += blockDim.x) {
+            const uint32_t bl = idx / K, kl = idx % K;
+            tile[kl * pitch + bl] = in[(uint64_t)(b0 + bl) * N + k0 + kl];
+        }
     }
     __syncthreads();
-    for (uint32_t idx = threadIdx.x; idx < kTrRows * kTrCols; idx += blockDim.x) {
-        const uint32_t kl = idx / kTrRows, bl = idx % kTrRows;
+#pragma unroll 4
+    for (uint32_t idx = threadIdx.x; idx < nb * K; idx += blockDim.x) {
+        const uint32_t kl = idx / nb, bl = idx % nb;
         const uint64_t k = k0 + kl;
-        if (b0 + bl < batches && k < N) {
-            const uint64_t r = lg_n ? (__brevll(k) >> (64 - lg_n)) : 0;
-            out[r * batches + b0 + bl] = tile[kl * (kTrRows + 1) + bl];
-        }
+        const uint64_t r = lg_n ? (__brevll(k) >> (64 - lg_n)) : 0;
+        out[r * batches + b0 + bl] = tile[kl * pitch + bl];
     }
 }
 
@@ -540,10 +558,20 @@ uint64_t ntt_scratch_elems(uint32_t lg, uint64_t batches) {
 void transpose_rev_run(uint64_t *out, const uint64_t *in, uint32_t lg_n, uint32_t batches, cudaStream_t s) {
     if (batches == 0) return;
     const uint64_t N = 1ull << lg_n;
-    const uint64_t gx = (N + kTrCols - 1) / kTrCols;
-    require(gx < (1ull << 31) && (batches + kTrRows - 1) / kTrRows < 65536, "transpose too large");
-    dim3 grid((unsigned)gx, (batches + kTrRows - 1) / kTrRows);
-    transpose_rev_kernel<<<grid, 256, 0, s>>>(out, in, lg_n, batches);
+    const uint64_t K = std::min<uint64_t>(N, kTrK);
+    const uint32_t nchunks = (batches + kTrMaxPolys - 1) / kTrMaxPolys;
+    const uint32_t chunk = (batches + nchunks - 1) / nchunks;  // balanced chunks
+    const uint64_t gx = N / K;
+    require(gx < (1ull << 31) && nchunks < 65536, "transpose too large");
+    const size_t smem = (size_t)K * (chunk | 1) * sizeof(uint64_t);
+    static std::atomic<uint64_t> attr_set{0};  // one bit per device
+    const int dev = current_device();
+    if (dev < 64 && !(attr_set.load() & (1ull << dev))) {
+        ZK_CUDA(cudaFuncSetAttribute(transpose_rev_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(kTrK * (kTrMaxPolys | 1) * sizeof(uint64_t))));
+        attr_set.fetch_or(1ull << dev);
+    }
+    transpose_rev_kernel<<<dim3((unsigned)gx, nchunks), 256, smem, s>>>(out, in, lg_n, batches, chunk);
     ZK_CHECK_LAUNCH();
 }
 
