@@ -38,6 +38,15 @@ HASH_NAMES = {"poseidon": 0, "keccak": 1, "poseidon2": 3}
 # Keccak-f 3720 64-bit logic ops counted as 2 each.
 OPS_PER_PERM = {0: 15378, 3: 7360, 1: 7440}
 
+# DRAM bytes (read + write) per step of each roofline's kernels, from one ncu
+# capture of this bench's default workload (profiles/ holds the commands and
+# figures); None for workloads that were not captured.
+NCU_TRAFFIC = {
+    ("merkle", 0, 135, 18): 331.5e6,      # merkle_leaves 317.9 MB + 4 wide levels 4.0 MB each + narrow levels
+    ("lde_leaves", 135, 18): 879.6e6,     # ntt_pass_kernel 258.4 MB + ntt_last_pass_leaves 621.2 MB
+    ("transpose", 135, 18): 531.4e6,      # transpose_rev_kernel
+}
+
 
 def set_workload(polys=135, lg_n=15, rate=3, cap_h=4, hash_name="poseidon", rot=4):
     """Workload of one step; the defaults are the plain single-job commit
@@ -350,7 +359,7 @@ def main() -> None:
             "achieved": ops / (t_mk * 1e-3) / 1e9,
             "peak": int_peak / 1e9 if int_peak else None,
             "frac": (ops / (t_mk * 1e-3)) / int_peak if int_peak else None,
-            "traffic": None,
+            "traffic": NCU_TRAFFIC.get(("merkle", HASH, B, LG)),
             "work_per_launch": f"{PERMS} {HASH_NAME} permutations x {OPS_PER_PERM[HASH]} INT32 multiply-class ops",
             "peak_source": "INT32 IMAD issue rate measured live by zeknox_b200/libzkprobe.so (MEASURED_PEAKS.json "
                            "has no integer figure)",
@@ -361,7 +370,15 @@ def main() -> None:
             "kernel": "LDE written as leaves (2 shared-memory NTT passes)", "bound": "hbm", "unit": "GB/s",
             "achieved": hbm_bytes / (t_lde * 1e-3) / 1e9, "peak": hbm_peak,
             "frac": (hbm_bytes / (t_lde * 1e-3) / 1e9) / hbm_peak if hbm_peak else None,
-            "traffic": None, "algorithmic_bytes": hbm_bytes, "ms_per_launch": t_lde,
+            "traffic": NCU_TRAFFIC.get(("lde_leaves", B, LG)), "algorithmic_bytes": hbm_bytes, "ms_per_launch": t_lde,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm_peak else None,
+        }
+        roof_tr = {
+            "kernel": "compute_transpose_rev (bit-reversing column -> leaf transpose, plain path)", "bound": "hbm",
+            "unit": "GB/s", "achieved": TRANSPOSE_BYTES / (p_tr * 1e-3) / 1e9, "peak": hbm_peak,
+            "frac": (TRANSPOSE_BYTES / (p_tr * 1e-3) / 1e9) / hbm_peak if hbm_peak else None,
+            "traffic": NCU_TRAFFIC.get(("transpose", B, LG)), "algorithmic_bytes": TRANSPOSE_BYTES,
+            "ms_per_launch": p_tr,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm_peak else None,
         }
         out = {
@@ -385,6 +402,7 @@ def main() -> None:
                                   "path": "zk_lde_async -> zk_transpose_rev_async -> zk_merkle_async"},
             "roofline": roof,
             "roofline_hbm": roof_hbm,
+            "roofline_transpose": roof_tr,
             "clocks": clk.summary(),
             "check": {"cap_device_path_equals_c_abi_path": bool(np.array_equal(cap_dev, cap_e2e))
                       if gpu_cap_input == e2e_input else None},
