@@ -61,6 +61,7 @@ struct PassArgs {
     const uint64_t *tw_lo, *tw_hi;  // omega_N powers (two-level)
     uint32_t tw_h;
     const uint64_t *line_roots;     // omega_4096^j, j < 4096
+    uint32_t inverse;               // direction of line_roots / tw (selects the DFT-8 constants)
 };
 
 __device__ __forceinline__ uint64_t pow2l(const uint64_t *lo, const uint64_t *hi, uint32_t h, uint64_t e) {
@@ -83,13 +84,61 @@ __device__ __forceinline__ void bfly1(uint64_t &u, uint64_t &v) {  // w = 1
     v = d;
 }
 
+// Multiplication by the 8th roots of unity.  In this field 2^96 = -1, so 2 has
+// order 192 and the 8th roots are powers of 2: for omega_8 = 7^((p-1)/8)
+// (the root every table here is built from), omega_8 = 2^120 = -2^24,
+// omega_8^2 = omega_4 = 2^48, omega_8^3 = -2^72, and the inverses are 2^72,
+// -2^48, 2^24.  x * 2^24 and x * 2^48 are a shift and one reduction, not a
+// 64 x 64 product; 2^72 stays a product with a constant.
+constexpr uint64_t kTwo72 = 0xffffffff00ull;  // 2^72 mod p = 2^40 - 2^8
+__device__ __forceinline__ uint64_t gl_mul2_24(uint64_t x) { return gl_reduce96(x << 24, (uint32_t)(x >> 40)); }
+__device__ __forceinline__ uint64_t gl_mul2_48(uint64_t x) { return gl_reduce128(x << 48, x >> 16); }
+
+// 8-point DFT in place (DIF radix-2 inside, natural order in, bit-reversed
+// out), with the direction's 8th roots.  Negated roots swap the operands of
+// the subtraction instead of negating.
+__device__ __forceinline__ void dft8(uint64_t x[8], bool inv) {
+    uint64_t d[4];
+    d[0] = gl_sub(x[0], x[4]);
+    if (!inv) {
+        d[1] = gl_mul2_24(gl_sub(x[5], x[1]));      // (x1 - x5) * (-2^24)
+        d[2] = gl_mul2_48(gl_sub(x[2], x[6]));      // (x2 - x6) * 2^48
+        d[3] = gl_mul(gl_sub(x[7], x[3]), kTwo72);  // (x3 - x7) * (-2^72)
+    } else {
+        d[1] = gl_mul(gl_sub(x[1], x[5]), kTwo72);  // * 2^72
+        d[2] = gl_mul2_48(gl_sub(x[6], x[2]));      // * (-2^48)
+        d[3] = gl_mul2_24(gl_sub(x[3], x[7]));      // * 2^24
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) x[k] = gl_add(x[k], x[k + 4]);
+#pragma unroll
+    for (int k = 0; k < 4; k++) x[k + 4] = d[k];
+    // span 2: (0,2), (1,3)*omega_4, (4,6), (5,7)*omega_4
+#pragma unroll
+    for (int h = 0; h < 8; h += 4) {
+        const uint64_t a0 = gl_add(x[h], x[h + 2]), a2 = gl_sub(x[h], x[h + 2]);
+        const uint64_t a1 = gl_add(x[h + 1], x[h + 3]);
+        const uint64_t a3 = inv ? gl_mul2_48(gl_sub(x[h + 3], x[h + 1])) : gl_mul2_48(gl_sub(x[h + 1], x[h + 3]));
+        // span 1
+        x[h] = gl_add(a0, a1);
+        x[h + 1] = gl_sub(a0, a1);
+        x[h + 2] = gl_add(a2, a3);
+        x[h + 3] = gl_sub(a2, a3);
+    }
+}
+
 // In-place DIF stages over T interleaved lines of length L = 2^l in shared
 // memory (element e of line t at e * tp + t), from half-span 2^s_top down to
-// 1: natural order in, bit-reversed out.  Stages are taken three at a time
-// (radix 8 in registers: one shared-memory round trip per three stages), then
-// a radix-4 or radix-2 tail.  tw[e] = omega_L^e for e < L.
+// 1: natural order in, bit-reversed out.  Stages are taken three at a time as
+// mixed-radix Cooley-Tukey steps: a sub-transform of size M = 8q splits into
+// 8-point DFTs over the elements o + j q (j < 8) followed by the twiddles
+// omega_M^(o * rev3(j)) on output j, then q-point sub-transforms; one
+// shared-memory round trip per step.  The 8-point DFTs multiply only by
+// powers of two (dft8), so a step costs 7 general products per 8 elements
+// instead of the 12 of three radix-2 stages, and the last step (q = 1) none.
+// A radix-4 or radix-2 tail ends odd stage counts.  tw[e] = omega_L^e.
 __device__ __forceinline__ void smem_dif(uint64_t *sm, const uint64_t *tw, uint32_t l, int s_top, uint32_t lg_t,
-                                         uint32_t tp) {
+                                         uint32_t tp, bool inv) {
     const uint32_t T = 1u << lg_t;
     int s = s_top;
     while (s >= 2) {  // spans 4q, 2q, q with q = 2^(s-2); unit = 8 elements at stride q
@@ -103,36 +152,30 @@ __device__ __forceinline__ void smem_dif(uint64_t *sm, const uint64_t *tw, uint3
             uint64_t x[8];
 #pragma unroll
             for (int k = 0; k < 8; k++) x[k] = sm[(e0 + k * q) * tp + t];
+            dft8(x, inv);
+            if (o != 0) {
+                constexpr uint32_t rev3[8] = {0, 4, 2, 6, 1, 5, 3, 7};
 #pragma unroll
-            for (int k = 0; k < 4; k++) bfly(x[k], x[k + 4], tw[(o + k * q) << sh8]);
-            const uint64_t w2a = tw[o << (sh8 + 1)], w2b = tw[(o + q) << (sh8 + 1)];
-            bfly(x[0], x[2], w2a);
-            bfly(x[1], x[3], w2b);
-            bfly(x[4], x[6], w2a);
-            bfly(x[5], x[7], w2b);
-            const uint64_t w1 = tw[o << (sh8 + 2)];
-#pragma unroll
-            for (int k = 0; k < 8; k += 2) bfly(x[k], x[k + 1], w1);
+                for (int j = 1; j < 8; j++) x[j] = gl_mul(x[j], tw[(o * rev3[j]) << sh8]);
+            }
 #pragma unroll
             for (int k = 0; k < 8; k++) sm[(e0 + k * q) * tp + t] = x[k];
         }
         s -= 3;
     }
     __syncthreads();
-    if (s == 1) {  // spans 2 and 1: radix-4 units
+    if (s == 1) {  // spans 2 and 1: radix-4 units (the 4th root is +-2^48)
         const uint32_t units = T << (l - 2);
         for (uint32_t u = threadIdx.x; u < units; u += blockDim.x) {
             const uint32_t t = u & (T - 1), e0 = (u >> lg_t) << 2;
-            uint64_t x0 = sm[e0 * tp + t], x1 = sm[(e0 + 1) * tp + t], x2 = sm[(e0 + 2) * tp + t],
-                     x3 = sm[(e0 + 3) * tp + t];
-            bfly1(x0, x2);
-            bfly(x1, x3, tw[(1u << l) >> 2]);  // omega_4
-            bfly1(x0, x1);
-            bfly1(x2, x3);
-            sm[e0 * tp + t] = x0;
-            sm[(e0 + 1) * tp + t] = x1;
-            sm[(e0 + 2) * tp + t] = x2;
-            sm[(e0 + 3) * tp + t] = x3;
+            const uint64_t x0 = sm[e0 * tp + t], x1 = sm[(e0 + 1) * tp + t], x2 = sm[(e0 + 2) * tp + t],
+                           x3 = sm[(e0 + 3) * tp + t];
+            const uint64_t a0 = gl_add(x0, x2), a2 = gl_sub(x0, x2), a1 = gl_add(x1, x3);
+            const uint64_t a3 = inv ? gl_mul2_48(gl_sub(x3, x1)) : gl_mul2_48(gl_sub(x1, x3));
+            sm[e0 * tp + t] = gl_add(a0, a1);
+            sm[(e0 + 1) * tp + t] = gl_sub(a0, a1);
+            sm[(e0 + 2) * tp + t] = gl_add(a2, a3);
+            sm[(e0 + 3) * tp + t] = gl_sub(a2, a3);
         }
         __syncthreads();
     } else if (s == 0) {  // span 1
@@ -193,7 +236,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
             for (uint32_t b = 1; b < (1u << rr); b++)
                 sm[((b << lv) + e) * tp + t] = gl_mul(v, tw[(e * brev_bits(b, rr)) & (L - 1)]);
         }
-        smem_dif(sm, tw, l, (int)lv - 1, a.lg_t, tp);
+        smem_dif(sm, tw, l, (int)lv - 1, a.lg_t, tp, a.inverse != 0);
         // store with the inter-pass twiddle w_N^((r0 + t) k Q), stepped by k
         const uint32_t t = threadIdx.x & (T - 1);
         const uint32_t k0 = threadIdx.x >> a.lg_t, dk = blockDim.x >> a.lg_t;
@@ -244,7 +287,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
         }
         sm[e * tp + t] = v;
     }
-    smem_dif(sm, tw, l, (int)l - 1, a.lg_t, tp);
+    smem_dif(sm, tw, l, (int)l - 1, a.lg_t, tp, a.inverse != 0);
     if (a.kind == 1) {
         // natural index of line t's element k: krev + Q * k
         uint64_t *dst = a.dst + poly0 * a.dst_poly_stride;
@@ -297,7 +340,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_last_pass_leaves(PassArgs a) 
         const uint32_t e = idx & (L - 1), p = idx >> l;
         sm[e * tp + p] = p < np ? a.src[(p0 + p) * a.src_poly_stride + (kpos << l) + e] : 0ull;
     }
-    smem_dif(sm, tw, l, (int)l - 1, a.lg_t, tp);
+    smem_dif(sm, tw, l, (int)l - 1, a.lg_t, tp, a.inverse != 0);
     const uint32_t lg = a.lg_n;
     for (uint32_t idx = threadIdx.x; idx < P * L; idx += blockDim.x) {
         const uint32_t p = idx & (P - 1), k = idx >> a.lg_t;
@@ -442,6 +485,7 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
     base.tw_hi = rt.hi();
     base.tw_h = rt.h;
     base.line_roots = lr;
+    base.inverse = j.inverse ? 1u : 0u;
     base.scale = j.scale;
     base.batches = j.batches;
     if (j.pre_coset) {
@@ -599,6 +643,7 @@ void ntt_run_on_tables(const NttJob &j, const PowTable &roots, const uint64_t *l
     base.tw_hi = roots.hi();
     base.tw_h = roots.h;
     base.line_roots = line_roots_dev;
+    base.inverse = j.inverse ? 1u : 0u;
     base.scale = j.scale;
     base.batches = j.batches;
     if (j.pre_coset) {
