@@ -52,13 +52,16 @@ struct PassArgs {
     // first pass: zero-extension and coset pre-multiply
     uint64_t n_valid;   // source elements per polynomial that are read (others are 0)
     const uint64_t *pre_lo, *pre_hi;  // coset powers (null: none)
+    const uint64_t *pre_full;         // the same powers in one table (null: two-level only)
     uint32_t pre_h;
     // last pass: output scaling by coset^k * scale
     const uint64_t *post_lo, *post_hi;  // coset powers (null: none)
+    const uint64_t *post_full;
     uint32_t post_h;
     uint64_t scale;     // 1 = none
     // twiddles
     const uint64_t *tw_lo, *tw_hi;  // omega_N powers (two-level)
+    const uint64_t *tw_full;        // omega_N^e for every e < N (null above 2^20 points)
     uint32_t tw_h;
     const uint64_t *line_roots;     // omega_4096^j, j < 4096
     uint32_t inverse;               // direction of line_roots / tw (selects the DFT-8 constants)
@@ -66,6 +69,11 @@ struct PassArgs {
 
 __device__ __forceinline__ uint64_t pow2l(const uint64_t *lo, const uint64_t *hi, uint32_t h, uint64_t e) {
     return gl_mul(__ldg(lo + (e & ((1ull << h) - 1))), __ldg(hi + (e >> h)));
+}
+// b^e from the one-load table when there is one, else from the two-level table.
+__device__ __forceinline__ uint64_t pow_at(const uint64_t *full, const uint64_t *lo, const uint64_t *hi, uint32_t h,
+                                           uint64_t e) {
+    return full ? __ldg(full + e) : pow2l(lo, hi, h, e);
 }
 
 __device__ __forceinline__ uint32_t brev_bits(uint32_t x, uint32_t bits) {
@@ -230,18 +238,26 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
             uint64_t v = 0;
             if (i < a.n_valid) {
                 v = gl_canon(src[i]);
-                if (a.pre_lo) v = gl_mul(v, pow2l(a.pre_lo, a.pre_hi, a.pre_h, i));
+                if (a.pre_lo) v = gl_mul(v, pow_at(a.pre_full, a.pre_lo, a.pre_hi, a.pre_h, i));
             }
             sm[e * tp + t] = v;
             for (uint32_t b = 1; b < (1u << rr); b++)
                 sm[((b << lv) + e) * tp + t] = gl_mul(v, tw[(e * brev_bits(b, rr)) & (L - 1)]);
         }
         smem_dif(sm, tw, l, (int)lv - 1, a.lg_t, tp, a.inverse != 0);
-        // store with the inter-pass twiddle w_N^((r0 + t) k Q), stepped by k
+        // store with the inter-pass twiddle w_N^((r0 + t) k Q): one table load
+        // each, or (no one-load table) stepped by k with a second product
         const uint32_t t = threadIdx.x & (T - 1);
         const uint32_t k0 = threadIdx.x >> a.lg_t, dk = blockDim.x >> a.lg_t;
         const uint64_t r = r0 + t;
         const uint64_t nmask = (1ull << a.lg_n) - 1;  // w_N has order N
+        if (a.tw_full) {
+            for (uint32_t k = k0; k < L; k += dk) {
+                const uint64_t tw_k = __ldg(a.tw_full + (((r * k) << a.lg_pre) & nmask));
+                dst[base + ((uint64_t)k << lg_s) + r] = gl_mul(sm[brev_bits(k, l) * tp + t], tw_k);
+            }
+            return;
+        }
         uint64_t twk = pow2l(a.tw_lo, a.tw_hi, a.tw_h, ((r * k0) << a.lg_pre) & nmask);
         const uint64_t step = pow2l(a.tw_lo, a.tw_hi, a.tw_h, ((r * dk) << a.lg_pre) & nmask);
         for (uint32_t k = k0; k < L; k += dk) {
@@ -279,7 +295,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
             if (a.kind == 2) {
                 if (e < a.n_valid) {
                     v = gl_canon(a.src[line_src(t) + e]);
-                    if (a.pre_lo) v = gl_mul(v, pow2l(a.pre_lo, a.pre_hi, a.pre_h, e));
+                    if (a.pre_lo) v = gl_mul(v, pow_at(a.pre_full, a.pre_lo, a.pre_hi, a.pre_h, e));
                 }
             } else {
                 v = a.src[line_src(t) + e];
@@ -295,7 +311,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
             const uint32_t t = idx & (T - 1), k = idx >> a.lg_t;
             uint64_t v = sm[brev_bits(k, l) * tp + t];
             const uint64_t o = c0 + t + ((uint64_t)k << a.lg_pre);
-            if (a.post_lo) v = gl_mul(v, pow2l(a.post_lo, a.post_hi, a.post_h, o));
+            if (a.post_lo) v = gl_mul(v, pow_at(a.post_full, a.post_lo, a.post_hi, a.post_h, o));
             if (a.scale != 1) v = gl_mul(v, a.scale);
             dst[o] = v;
         }
@@ -312,7 +328,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
             const uint32_t k = idx & (L - 1), t = idx >> l;
             if (t >= nlines) continue;
             uint64_t v = sm[brev_bits(k, l) * tp + t];
-            if (a.post_lo) v = gl_mul(v, pow2l(a.post_lo, a.post_hi, a.post_h, k));
+            if (a.post_lo) v = gl_mul(v, pow_at(a.post_full, a.post_lo, a.post_hi, a.post_h, k));
             if (a.scale != 1) v = gl_mul(v, a.scale);
             a.dst[(poly0 + t) * a.dst_poly_stride + k] = v;
         }
@@ -484,6 +500,7 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
     base.tw_lo = rt.lo();
     base.tw_hi = rt.hi();
     base.tw_h = rt.h;
+    base.tw_full = rt.full;
     base.line_roots = lr;
     base.inverse = j.inverse ? 1u : 0u;
     base.scale = j.scale;
@@ -492,11 +509,13 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
         base.pre_lo = j.pre_coset->lo();
         base.pre_hi = j.pre_coset->hi();
         base.pre_h = j.pre_coset->h;
+        base.pre_full = j.pre_coset->full;
     }
     if (j.post_coset) {
         base.post_lo = j.post_coset->lo();
         base.post_hi = j.post_coset->hi();
         base.post_h = j.post_coset->h;
+        base.post_full = j.post_coset->full;
     }
 
     if (plan.passes == 1) {
@@ -650,11 +669,13 @@ void ntt_run_on_tables(const NttJob &j, const PowTable &roots, const uint64_t *l
         base.pre_lo = j.pre_coset->lo();
         base.pre_hi = j.pre_coset->hi();
         base.pre_h = j.pre_coset->h;
+        base.pre_full = j.pre_coset->full;
     }
     if (j.post_coset) {
         base.post_lo = j.post_coset->lo();
         base.post_hi = j.post_coset->hi();
         base.post_h = j.post_coset->h;
+        base.post_full = j.post_coset->full;
     }
     if (plan.passes == 1) {
         PassArgs a = base;

@@ -62,6 +62,15 @@ PowTable make_pow_table(uint64_t base, unsigned bits) {
     uint64_t y = 1;
     for (uint64_t i = 0; i < nhi; i++, y = h_mul(y, step)) v[nlo + i] = y;
     t.dev = upload(v);
+    if (bits <= kFullTableMaxLg) {
+        std::vector<uint64_t> f(1ull << bits);
+        uint64_t z = 1;
+        for (auto &e : f) {
+            e = z;
+            z = h_mul(z, base);
+        }
+        t.full = upload(f);
+    }
     return t;
 }
 }  // namespace
@@ -133,7 +142,8 @@ const PowTable &coset_table(DeviceCtx &c, unsigned lg, uint64_t gen, bool replac
         if (t.dev) {
             ZK_CUDA(cudaDeviceSynchronize());  // no kernel may still read the old table
             cudaFree(t.dev);
-            t.dev = nullptr;
+            if (t.full) cudaFree(t.full);
+            t.dev = t.full = nullptr;
         }
         t = make_pow_table(want_gen, want_bits);
     }

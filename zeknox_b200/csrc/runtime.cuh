@@ -66,6 +66,7 @@ constexpr uint64_t GROUP_GENERATOR = 7;  // native/ff/gl64_params.hpp:12
 // for e < 2^bits.  Both halves live in one device allocation.
 struct PowTable {
     uint64_t *dev = nullptr;  // [lo (2^h) | hi (2^(bits-h))]
+    uint64_t *full = nullptr; // b^e for every e < 2^bits when bits <= kFullTableMaxLg, else null
     unsigned bits = 0, h = 0;
     uint64_t base = 0;
     const uint64_t *lo() const { return dev; }
@@ -73,6 +74,7 @@ struct PowTable {
 };
 
 constexpr int kMaxLg = 32;
+constexpr unsigned kFullTableMaxLg = 20;  // one-load power tables up to 2^20 entries (8 MB)
 constexpr int kLineLgMax = 12;  // longest in-shared-memory line: 4096 elements
 
 // Per-device state.  Tables are built lazily, under `mu`.
