@@ -575,11 +575,12 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
                 const uint64_t groups = nb << (lg - a.l - a.lg_t);
                 launch_pass(a, groups, s);
             } else if (j.to_leaves) {
-                // 16 polynomials per block: 128-byte runs in every leaf row
+                // 8 polynomials per block: 64-byte runs in every leaf row (more resident
+                // blocks hide the loads of the intermediate better than 16 did)
                 a.kind = 3;
                 a.lg_s = 0;
                 a.lg_pre = lg - a.l;
-                a.lg_t = a.l <= 9 ? 4 : 13 - a.l;
+                a.lg_t = a.l <= 9 ? 3 : 12 - a.l;
                 a.src = scr;
                 a.src_poly_stride = N;
                 a.dst = j.dst + b0;
