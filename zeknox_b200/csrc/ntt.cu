@@ -92,6 +92,14 @@ __device__ __forceinline__ void bfly1(uint64_t &u, uint64_t &v) {  // w = 1
     v = d;
 }
 
+// 8-byte asynchronous global -> shared copy (cp.async, no register staging),
+// so a thread's loads of a tile are all in flight at once.
+__device__ __forceinline__ void cp_async8(uint64_t *smem_dst, const uint64_t *gmem_src) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Multiplication by the 8th roots of unity.  In this field 2^96 = -1, so 2 has
 // order 192 and the 8th roots are powers of 2: for omega_8 = 7^((p-1)/8)
 // (the root every table here is built from), omega_8 = 2^120 = -2^24,
@@ -298,11 +306,13 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
                     if (a.pre_lo) v = gl_mul(v, pow_at(a.pre_full, a.pre_lo, a.pre_hi, a.pre_h, e));
                 }
             } else {
-                v = a.src[line_src(t) + e];
+                cp_async8(&sm[e * tp + t], a.src + line_src(t) + e);
+                continue;
             }
         }
         sm[e * tp + t] = v;
     }
+    cp_async_wait_all();
     smem_dif(sm, tw, l, (int)l - 1, a.lg_t, tp, a.inverse != 0);
     if (a.kind == 1) {
         // natural index of line t's element k: krev + Q * k
@@ -354,8 +364,10 @@ __global__ void __launch_bounds__(kNttThreads) ntt_last_pass_leaves(PassArgs a) 
     const uint64_t kpos = ((krev & mask1) << (a.lg_pre - a.l_first)) | (krev >> a.l_first);
     for (uint32_t idx = threadIdx.x; idx < P * L; idx += blockDim.x) {
         const uint32_t e = idx & (L - 1), p = idx >> l;
-        sm[e * tp + p] = p < np ? a.src[(p0 + p) * a.src_poly_stride + (kpos << l) + e] : 0ull;
+        if (p < np) cp_async8(&sm[e * tp + p], a.src + (p0 + p) * a.src_poly_stride + (kpos << l) + e);
+        else sm[e * tp + p] = 0ull;
     }
+    cp_async_wait_all();
     smem_dif(sm, tw, l, (int)l - 1, a.lg_t, tp, a.inverse != 0);
     const uint32_t lg = a.lg_n;
     for (uint32_t idx = threadIdx.x; idx < P * L; idx += blockDim.x) {
