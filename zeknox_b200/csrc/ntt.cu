@@ -240,13 +240,34 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
         }
         const uint32_t rr = l - lv;
         __syncthreads();
+        if (rr >= 2) {
+            // Stage the inputs (block 1 of the line) and their coset powers
+            // (block 2) with asynchronous copies, so all of a thread's loads are
+            // in flight together; each thread reads back only the slots it
+            // staged, before its own replication overwrites them.
+            for (uint32_t idx = threadIdx.x; idx < (T << lv); idx += blockDim.x) {
+                const uint32_t t = idx & (T - 1), e = idx >> a.lg_t;
+                const uint64_t i = base + ((uint64_t)e << lg_s) + r0 + t;
+                if (i < a.n_valid) {
+                    cp_async8(&sm[((1u << lv) + e) * tp + t], src + i);
+                    if (a.pre_full) cp_async8(&sm[((2u << lv) + e) * tp + t], a.pre_full + i);
+                }
+            }
+            cp_async_wait_all();
+        }
         for (uint32_t idx = threadIdx.x; idx < (T << lv); idx += blockDim.x) {
             const uint32_t t = idx & (T - 1), e = idx >> a.lg_t;
             const uint64_t i = base + ((uint64_t)e << lg_s) + r0 + t;  // index within the polynomial
             uint64_t v = 0;
             if (i < a.n_valid) {
-                v = gl_canon(src[i]);
-                if (a.pre_lo) v = gl_mul(v, pow_at(a.pre_full, a.pre_lo, a.pre_hi, a.pre_h, i));
+                if (rr >= 2) {
+                    v = gl_canon(sm[((1u << lv) + e) * tp + t]);
+                    if (a.pre_full) v = gl_mul(v, sm[((2u << lv) + e) * tp + t]);
+                    else if (a.pre_lo) v = gl_mul(v, pow2l(a.pre_lo, a.pre_hi, a.pre_h, i));
+                } else {
+                    v = gl_canon(src[i]);
+                    if (a.pre_lo) v = gl_mul(v, pow_at(a.pre_full, a.pre_lo, a.pre_hi, a.pre_h, i));
+                }
             }
             sm[e * tp + t] = v;
             for (uint32_t b = 1; b < (1u << rr); b++)
