@@ -7,7 +7,8 @@
  *
  * Parity is pinned (tests/test_oracle.py) against
  *   - the known-answer vectors of zeknox's own tests (native/tests/tests.cu
- *     Poseidon :279-292, Poseidon2 :409-428, Keccak :164-173; Go Merkle caps
+ *     Poseidon :279-292, Poseidon2 :409-428, Keccak :164-173, Monolith
+ *     :201-203; Go Merkle caps
  *     wrappers/go/lib/lib_test.go:194-213), committed in tests/golden/, and
  *   - outputs of zeknox's own C++ CPU Merkle path compiled from its sources
  *     (oracle/build_ref.sh -> oracle/_ref/), committed as fixtures.
@@ -185,8 +186,61 @@ void orc_keccak256(const uint8_t *in, size_t len, uint8_t out[32]) {
     memcpy(out, st, 32);
 }
 
+/* --------------------------------------------------------------- Monolith */
+/* monolith/monolith.cu:117-233 (Monolith-64, width 12, 6 rounds):
+ * state = (lo, hi) with hi in {0, 1} (a 65-bit lane); concrete(rc) sets lane r
+ * to (sum_c M[r][c] (lo_c + 2^64 hi_c) + rc[r]) mod p, canonical, hi = 0, with
+ * M circulant (row r column c = ROW[(c - r) mod 12]); bars apply the byte-wise
+ * Bar S-box to lanes 0..3 (per byte: y = rotl1(x ^ (rotl1(~x) & rotl2(x) &
+ * rotl3(x)))); bricks (Feistel type 3) add, from lane 11 down to lane 1, the
+ * square mod p of the lane below (its value before the layer) as a 64-bit sum
+ * whose carry goes to hi.  Permutation: concrete(rc0); then for r = 1..6
+ * bars, bricks, concrete(rc_r). */
+static u64 mono_rotl_bytes(u64 x, int k) {
+    u64 out = 0;
+    for (int b = 0; b < 8; b++) {
+        unsigned v = (unsigned)(x >> (8 * b)) & 0xff;
+        v = ((v << k) | (v >> (8 - k))) & 0xff;
+        out |= (u64)v << (8 * b);
+    }
+    return out;
+}
+static u64 mono_bar(u64 x) {
+    u64 t = x ^ (mono_rotl_bytes(~x, 1) & mono_rotl_bytes(x, 2) & mono_rotl_bytes(x, 3));
+    return mono_rotl_bytes(t, 1);
+}
+static void mono_concrete(u64 lo[12], unsigned hi[12], const u64 *rc) {
+    u64 out[12];
+    for (int r = 0; r < 12; r++) {
+        u128 acc = rc[r];
+        for (int c = 0; c < 12; c++) {
+            u128 m = ZK_MONOLITH_MDS_ROW[(c - r + 12) % 12];
+            acc += m * lo[c] + ((m * hi[c]) << 64);
+        }
+        out[r] = red128(acc);
+    }
+    for (int r = 0; r < 12; r++) {
+        lo[r] = out[r];
+        hi[r] = 0;
+    }
+}
+void orc_monolith_permute(u64 st[12]) {
+    unsigned hi[12] = {0};
+    mono_concrete(st, hi, ZK_MONOLITH_RC);
+    for (int r = 1; r <= 6; r++) {
+        for (int i = 0; i < 4; i++) st[i] = mono_bar(st[i]);
+        for (int i = 11; i > 0; i--) {
+            u64 sq = orc_mul(st[i - 1], st[i - 1]);
+            u64 s = st[i] + sq;
+            hi[i] = s < sq;
+            st[i] = s;
+        }
+        mono_concrete(st, hi, ZK_MONOLITH_RC + 12 * r);
+    }
+}
+
 /* ---------------------------------------------------------------- hashers */
-enum { H_POSEIDON = 0, H_KECCAK = 1, H_POSEIDON2 = 3 };
+enum { H_POSEIDON = 0, H_KECCAK = 1, H_POSEIDON2 = 3, H_MONOLITH = 4 };
 
 /* Sponge of poseidon/poseidon_permutation.cuh:226-276 (GPU) and
  * poseidon_permutation.hpp:84-139 (CPU): width 12, rate 8, overwrite mode.
@@ -238,6 +292,7 @@ int orc_hash_one(int ht, const u64 *in, u64 n, u64 out[4]) {
     switch (ht) {
     case H_POSEIDON: sponge_hash_one(orc_poseidon_permute, in, n, out); return 0;
     case H_POSEIDON2: sponge_hash_one(orc_poseidon2_permute, in, n, out); return 0;
+    case H_MONOLITH: sponge_hash_one(orc_monolith_permute, in, n, out); return 0;
     case H_KECCAK: keccak_hash_one(in, n, out); return 0;
     default: return -1;
     }
@@ -246,6 +301,7 @@ int orc_hash_two(int ht, const u64 *l, const u64 *r, u64 out[4]) {
     switch (ht) {
     case H_POSEIDON: sponge_hash_two(orc_poseidon_permute, l, r, out); return 0;
     case H_POSEIDON2: sponge_hash_two(orc_poseidon2_permute, l, r, out); return 0;
+    case H_MONOLITH: sponge_hash_two(orc_monolith_permute, l, r, out); return 0;
     case H_KECCAK: keccak_hash_two(l, r, out); return 0;
     default: return -1;
     }
@@ -263,7 +319,7 @@ int orc_hash_two(int ht, const u64 *l, const u64 *r, u64 out[4]) {
  *    H2(node 0, node 1). */
 int orc_merkle_fill(u64 *digests, u64 *cap, const u64 *leaves, u64 n_digests, u64 n_caps,
                     u64 n_leaves, u64 leaf_size, u64 cap_height, int ht) {
-    if (ht != H_POSEIDON && ht != H_POSEIDON2 && ht != H_KECCAK) return -1;
+    if (ht != H_POSEIDON && ht != H_POSEIDON2 && ht != H_KECCAK && ht != H_MONOLITH) return -1;
     if (n_caps == n_leaves) {
 #pragma omp parallel for schedule(static)
         for (long long i = 0; i < (long long)n_leaves; i++)

@@ -54,6 +54,7 @@ def lib():
             getattr(L, name).restype = u64
         L.orc_poseidon_permute.argtypes = [_u64p]
         L.orc_poseidon2_permute.argtypes = [_u64p]
+        L.orc_monolith_permute.argtypes = [_u64p]
         L.orc_keccak256.argtypes = [vp, ctypes.c_size_t, vp]
         L.orc_hash_one.argtypes = [c_int, _u64p, u64, _u64p]
         L.orc_hash_one.restype = c_int
@@ -129,7 +130,9 @@ def hash_two(ht: int, left: np.ndarray, right: np.ndarray) -> np.ndarray:
 def permute(ht: int, state: np.ndarray) -> np.ndarray:
     st = np.ascontiguousarray(state, dtype=np.uint64).copy()
     assert st.size == 12
-    (lib().orc_poseidon_permute if ht == HASH_POSEIDON else lib().orc_poseidon2_permute)(_ptr(st))
+    perm = {HASH_POSEIDON: lib().orc_poseidon_permute, HASH_POSEIDON2: lib().orc_poseidon2_permute,
+            HASH_MONOLITH: lib().orc_monolith_permute}[ht]
+    perm(_ptr(st))
     return st
 
 

@@ -5,8 +5,9 @@ kat.json
     Known-answer vectors transcribed from zeknox's own tests, with the file and
     line each one comes from (parsed from those files, not typed in):
     Poseidon hash_one sizes 1..9 (native/tests/tests.cu:279-292), Poseidon2
-    Fibonacci input (tests.cu:409-428), Keccak sizes 1..6 (tests.cu:164-173) and
-    the Go Merkle caps (wrappers/go/lib/lib_test.go:194-213).
+    Fibonacci input (tests.cu:409-428), Keccak sizes 1..6 (tests.cu:164-173),
+    Monolith hash_one of 0..11 (tests.cu:201-203) and the Go Merkle caps
+    (wrappers/go/lib/lib_test.go:194-213).
 
 merkle_ref_cpu.npz
     Digests and caps produced by zeknox's own C++ CPU Merkle path
@@ -34,7 +35,8 @@ MERKLE_SHAPES = [
     (8, 7, 3), (16, 9, 4), (8, 7, 2), (16, 7, 1), (64, 135, 2), (256, 9, 0), (1024, 16, 4),
     (32, 4, 1), (32, 3, 1), (128, 8, 3), (512, 13, 2), (256, 135, 4),
 ]
-HASHES = {"poseidon": O.HASH_POSEIDON, "poseidon2": O.HASH_POSEIDON2, "keccak": O.HASH_KECCAK}
+HASHES = {"poseidon": O.HASH_POSEIDON, "poseidon2": O.HASH_POSEIDON2, "keccak": O.HASH_KECCAK,
+          "monolith": O.HASH_MONOLITH}
 
 
 def _u64s(txt):
@@ -62,6 +64,10 @@ def parse_kats(zk: Path) -> dict:
     kexp = [_u64s(l) for l in tests[166:173] if "{" in l]
     kat["keccak_hash_one"] = {"source": "native/tests/tests.cu:164-173", "data": data,
                               "expected": {str(s): kexp[s] for s in range(1, 7)}}
+    # Monolith: input at tests.cu:203, expected digest at :204.
+    mono_in = _u64s(block(tests, 203, 203).split("=", 1)[1])
+    mono_exp = _u64s(block(tests, 204, 204).split("=", 1)[1])
+    kat["monolith_hash_one"] = {"source": "native/tests/tests.cu:201-204", "input": mono_in, "expected": mono_exp}
     # Go caps: leaf at lib_test.go:195, three (nLeaves, nCaps, expHash) cases.
     gl = _u64s(block(gotest, 195, 195).split("{", 1)[1])
     cases = []
@@ -72,6 +78,7 @@ def parse_kats(zk: Path) -> dict:
         cases.append({"n_leaves": nl, "n_caps": nc, "cap": _u64s(eh)})
     kat["go_merkle_caps"] = {"source": "wrappers/go/lib/lib_test.go:194-213", "leaf": gl, "cases": cases}
     assert len(cases) == 3 and len(exp) >= 10 and len(kexp) == 7 and len(p2) == 4
+    assert len(mono_in) == 12 and len(mono_exp) == 4
     return kat
 
 

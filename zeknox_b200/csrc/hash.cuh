@@ -8,6 +8,7 @@
 //   Poseidon2  native/poseidon2/poseidon2.cu:61-209
 //   Keccak     native/keccak/keccak.cu:42-135 (rate 136 B, 0x01 .. 0x80 pad,
 //              digest word 3 masked to its low byte)
+//   Monolith   native/monolith/monolith.cu:117-233
 //   sponge     native/poseidon/poseidon_permutation.cuh:226-276 (rate 8,
 //              overwrite mode, n <= 4 copies and zero-pads)
 #pragma once
@@ -150,8 +151,17 @@ __host__ __device__ constexpr int mds_q2(int r, int k) {  // A - B, plus d on (0
 }
 #undef ZK_MDS_TABLES
 
-// One half-vector: a[i] = 2^52 + x[i] in, o[r] = k[r] + (MDS x)[r] out.
-__device__ __forceinline__ void poseidon_mds_half(const double a[12], double o[12], const double *k) {
+// Coefficients of the circulant split for one hasher's MDS.
+struct PoseidonCirc {
+    __host__ __device__ static constexpr int p2(int r, int k) { return mds_p2(r, k); }
+    __host__ __device__ static constexpr int q2(int r, int k) { return mds_q2(r, k); }
+    __host__ __device__ static constexpr int d0() { return mds_diag0(); }
+};
+
+// One half-vector: a[i] = 2^52 + x[i] in, o[r] = k[r] + (M x)[r] out, M the
+// circulant (plus diag(d0, 0, ...)) of C.
+template <class C>
+__device__ __forceinline__ void circ12_half(const double a[12], double o[12], const double *k) {
     double u[6], w[6], x6 = 0.0;
 #pragma unroll
     for (int i = 0; i < 6; i++) {
@@ -164,21 +174,26 @@ __device__ __forceinline__ void poseidon_mds_half(const double a[12], double o[1
     for (int r = 0; r < 6; r++) {
         // Lanes 0 and 6 (u[0], w[0]) last: in a partial round only lane 0 has
         // just left the S-box, so the other terms need not wait for it.
-        double pa = (double)mds_p2(r, 1) * u[1], qa = (double)mds_q2(r, 1) * w[1];
+        double pa = (double)C::p2(r, 1) * u[1], qa = (double)C::q2(r, 1) * w[1];
 #pragma unroll
         for (int c = 2; c < 6; c++) {
-            pa = fma((double)mds_p2(r, c), u[c], pa);
-            qa = fma((double)mds_q2(r, c), w[c], qa);
+            pa = fma((double)C::p2(r, c), u[c], pa);
+            qa = fma((double)C::q2(r, c), w[c], qa);
         }
-        pa = fma((double)mds_p2(r, 0), u[0], pa);
-        qa = fma((double)mds_q2(r, 0), w[0], qa);
+        pa = fma((double)C::p2(r, 0), u[0], pa);
+        qa = fma((double)C::q2(r, 0), w[0], qa);
         // The (0, 0) terms carry d (u + w) = 2 d x_lo[0] into lane 0; lane 6
         // must not get d (u - w) = 2 d x_hi[0], so it is taken out again.
         double d = pa - qa;
-        if (r == 0) d = fma(-2.0 * (double)mds_diag0(), x6, d);
+        if constexpr (C::d0() != 0) {
+            if (r == 0) d = fma(-2.0 * (double)C::d0(), x6, d);
+        }
         o[r] = fma(0.5, pa + qa, k[r]);
         o[r + 6] = fma(0.5, d, k[r + 6]);
     }
+}
+__device__ __forceinline__ void poseidon_mds_half(const double a[12], double o[12], const double *k) {
+    circ12_half<PoseidonCirc>(a, o, k);
 }
 
 // s <- MDS s + c, c being round rnd + 1's constants (none after round 29).
@@ -352,8 +367,91 @@ __device__ __forceinline__ void keccak_f1600(uint64_t a[25]) {
     }
 }
 
+// --------------------------------------------------------------- Monolith
+// Monolith-64, width 12, 6 rounds (native/monolith/monolith.cu:117-233):
+// concrete(rc_0), then per round r = 1..6: bars, bricks, concrete(rc_r).
+//  * concrete: the circulant matrix (row r column c = ROW[(c - r) mod 12], row
+//    sum 160) plus the round constant, mod p.  The same exact FP64 split as
+//    the Poseidon MDS, no diagonal.  Lanes 0-3 are canonicalised afterwards:
+//    the Bar S-box acts on the bits of the canonical value.
+//  * bars: Bar on every byte of lanes 0-3,
+//    y = rotl1(x ^ (rotl1(~x) & rotl2(x) & rotl3(x))) (rotations within the byte).
+//  * bricks (Feistel type 3): lane i, from 11 down to 1, += (lane i-1)^2 mod p,
+//    the square of lane i-1 before the layer.  zeknox keeps that sum as a
+//    65-bit value for the next concrete layer; here it is taken mod p
+//    (pr_add_c), which is the same field element.
+#define ZK_MONO_ROW constexpr uint32_t row[12] = {ZK_MONOLITH_MDS_ROW_LIST};
+struct MonolithCirc {
+    __host__ __device__ static constexpr int p2(int r, int k) {
+        ZK_MONO_ROW
+        return (int)(row[(k - r + 12) % 12] + row[(k + 6 - r + 12) % 12]);
+    }
+    __host__ __device__ static constexpr int q2(int r, int k) {
+        ZK_MONO_ROW
+        return (int)row[(k - r + 12) % 12] - (int)row[(k + 6 - r + 12) % 12];
+    }
+    __host__ __device__ static constexpr int d0() { return 0; }
+};
+#undef ZK_MONO_ROW
+
+// Accumulator starting values of the 7 concrete layers ("to integers" form:
+// 2^52 + the 32-bit halves of (rc - kMagicAdj) mod p).
+struct MonolithTab {
+    double k[7][2][12];
+};
+constexpr MonolithTab make_monolith_tab() {
+    MonolithTab t{};
+    constexpr uint64_t rc[84] = {ZK_MONOLITH_RC_LIST};
+    for (int rnd = 0; rnd < 7; rnd++)
+        for (int r = 0; r < 12; r++) {
+            const uint64_t m = cx_sub_mod(cx_canon(rc[12 * rnd + r]), kMagicAdj);
+            t.k[rnd][0][r] = kMagic + (double)(m & 0xffffffffull);
+            t.k[rnd][1][r] = kMagic + (double)(m >> 32);
+        }
+    return t;
+}
+__constant__ MonolithTab c_monolith = make_monolith_tab();
+__device__ MonolithTab g_monolith = make_monolith_tab();
+
+__device__ __forceinline__ void monolith_concrete(uint64_t s[12], const double (*k)[12]) {
+    double a[12], lo[12], hi[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) a[i] = magic_in((uint32_t)s[i]);
+    circ12_half<MonolithCirc>(a, lo, k[0]);
+#pragma unroll
+    for (int i = 0; i < 12; i++) a[i] = magic_in((uint32_t)(s[i] >> 32));
+    circ12_half<MonolithCirc>(a, hi, k[1]);
+#pragma unroll
+    for (int r = 0; r < 12; r++) s[r] = pr_reduce_split_nc(magic_out(lo[r]), magic_out(hi[r]));
+#pragma unroll
+    for (int r = 0; r < 4; r++) s[r] = gl_canon(s[r]);
+}
+
+// Rotate every byte of x left by K (within the byte).
+template <int K>
+__device__ __forceinline__ uint32_t rotl_bytes(uint32_t x) {
+    constexpr uint32_t low = 0x01010101u * ((1u << K) - 1u);  // the low K bits of each byte
+    return ((x << K) & ~low) | ((x >> (8 - K)) & low);
+}
+__device__ __forceinline__ uint32_t monolith_bar32(uint32_t x) {
+    return rotl_bytes<1>(x ^ (rotl_bytes<1>(~x) & rotl_bytes<2>(x) & rotl_bytes<3>(x)));
+}
+
+__device__ __forceinline__ void monolith_permute(uint64_t s[12], const MonolithTab &tab = c_monolith) {
+    monolith_concrete(s, tab.k[0]);
+#pragma unroll 1
+    for (int rnd = 1; rnd <= 6; rnd++) {
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            s[i] = ((uint64_t)monolith_bar32((uint32_t)(s[i] >> 32)) << 32) | monolith_bar32((uint32_t)s[i]);
+#pragma unroll
+        for (int i = 11; i > 0; i--) s[i] = pr_add_c(s[i], gl_mul(s[i - 1], s[i - 1]));
+        monolith_concrete(s, tab.k[rnd]);
+    }
+}
+
 // ------------------------------------------------------------ hashers
-enum : int { kPoseidon = 0, kKeccak = 1, kPoseidon2 = 3 };
+enum : int { kPoseidon = 0, kKeccak = 1, kPoseidon2 = 3, kMonolith = 4 };
 
 // Leaf elements are reduced mod p when read (a no-op for canonical inputs).
 template <int H, int W = 4>
@@ -407,6 +505,7 @@ __device__ __forceinline__ void hash_one(const uint64_t *__restrict__ in, uint32
                     if ((uint32_t)j < len) s[j] = gl_canon(in[idx + j]);
             }
             if constexpr (H == kPoseidon) poseidon_permute<W>(s);
+            else if constexpr (H == kMonolith) monolith_permute(s);
             else poseidon2_permute<W>(s);
         }
         out[0] = gl_canon(s[0]);
@@ -430,10 +529,15 @@ template <>
 struct TabOf<kKeccak> {
     using type = KeccakTab;
 };
+template <>
+struct TabOf<kMonolith> {
+    using type = MonolithTab;
+};
 template <int H>
 __device__ __forceinline__ const typename TabOf<H>::type &const_tab() {
     if constexpr (H == kPoseidon) return c_poseidon;
     else if constexpr (H == kPoseidon2) return c_poseidon2;
+    else if constexpr (H == kMonolith) return c_monolith;
     else return c_keccak_tab;
 }
 
@@ -442,6 +546,7 @@ template <int H>
 __device__ __forceinline__ const typename TabOf<H>::type *global_tab() {
     if constexpr (H == kPoseidon) return &g_poseidon;
     else if constexpr (H == kPoseidon2) return &g_poseidon2;
+    else if constexpr (H == kMonolith) return &g_monolith;
     else return nullptr;
 }
 
@@ -477,6 +582,7 @@ __device__ __forceinline__ void hash_two(const uint64_t *l, const uint64_t *r, u
             s[8 + i] = 0;
         }
         if constexpr (H == kPoseidon) poseidon_permute<W>(s, tab);
+        else if constexpr (H == kMonolith) monolith_permute(s, tab);
         else poseidon2_permute<W>(s, tab);
         out[0] = gl_canon(s[0]);
         out[1] = gl_canon(s[1]);

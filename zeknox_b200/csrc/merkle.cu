@@ -244,7 +244,9 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
 
 }  // namespace
 
-bool merkle_hash_supported(uint64_t ht) { return ht == kPoseidon || ht == kPoseidon2 || ht == kKeccak; }
+bool merkle_hash_supported(uint64_t ht) {
+    return ht == kPoseidon || ht == kPoseidon2 || ht == kKeccak || ht == kMonolith;
+}
 
 void merkle_validate(const MerkleJob &j) {
     require(merkle_hash_supported(j.hash_type), "unsupported hash type " + std::to_string(j.hash_type));
@@ -265,6 +267,7 @@ void merkle_run(const MerkleJob &j, cudaStream_t st) {
     case kPoseidon: merkle_run_t<kPoseidon>(j, st); break;
     case kPoseidon2: merkle_run_t<kPoseidon2>(j, st); break;
     case kKeccak: merkle_run_t<kKeccak>(j, st); break;
+    case kMonolith: merkle_run_t<kMonolith>(j, st); break;
     default: break;
     }
 }
