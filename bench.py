@@ -32,7 +32,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Goldilocks LDE+Merkle commit elems/s, batched vs plain, bit-exact; p99 latency"
 P = 0xFFFFFFFF00000001
-HASH_NAMES = {"poseidon": 0, "keccak": 1, "poseidon2": 3, "monolith": 4}
+HASH_NAMES = {"poseidon": 0, "keccak": 1, "poseidonbn128": 2, "poseidon2": 3, "monolith": 4}
 # INT32 multiply-class ops per permutation (a 64x64 mulmod counts 10, a
 # small-constant MAC 4): Poseidon 1077 mulmod + 1152 MAC, Poseidon2 736 mulmod,
 # Keccak-f 3720 64-bit logic ops counted as 2 each, Monolith 66 mulmod (bricks)
@@ -471,7 +471,7 @@ def run_merkle_only(args):
 
 
 def run_sweep(args):
-    """Hash sweep: 2^20 leaves x 135, cap height 4, Poseidon / Poseidon2 / Keccak / Monolith."""
+    """Hash sweep: 2^20 leaves x 135, cap height 4, Poseidon / Poseidon2 / Keccak / Monolith / Poseidon-BN128."""
     import torch
 
     import zeknox_b200 as zk
@@ -480,22 +480,22 @@ def run_sweep(args):
     leaves = _device_pool(torch, nl * w, 0x5EED0004).view(nl, w)
     peak = int32_peak()
     res = {"workload": "merkle sweep 2^20 x 135, cap_height 4", "int32_peak_gops": peak / 1e9 if peak else None}
-    for name, ht in (("poseidon", 0), ("poseidon2", 3), ("keccak", 1), ("monolith", 4)):
+    for name, ht in (("poseidon", 0), ("poseidon2", 3), ("keccak", 1), ("monolith", 4), ("poseidonbn128", 2)):
         d, c = zk.merkle_tree(leaves, ch, ht)
         for _ in range(args.warmup):
             zk.merkle_tree(leaves, ch, ht, d, c)
         ms = _ev_ms(torch, lambda: zk.merkle_tree(leaves, ch, ht, d, c), max(3, args.steps // 4))
         rate_words = 17 if ht == 1 else 8
         perms = nl * ((w + rate_words - 1) // rate_words) + nl
-        ops = perms * OPS_PER_PERM[ht]
+        ops = perms * OPS_PER_PERM.get(ht, 0)
         res[name] = {"ms": ms, "perm_per_s": perms / (ms * 1e-3), "leaf_elems_per_s": nl * w / (ms * 1e-3),
-                     "int32_frac": ops / (ms * 1e-3) / peak if peak else None}
+                     "int32_frac": ops / (ms * 1e-3) / peak if peak and ht in OPS_PER_PERM else None}
     # zeknox's CPU path on a 2^14-leaf sample of the same shape
     from oracle import oracle as O
 
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
     sample = leaves[: 1 << 14].cpu().numpy().reshape(-1)
-    for name, ht in (("poseidon", 0), ("poseidon2", 3), ("keccak", 1), ("monolith", 4)):
+    for name, ht in (("poseidon", 0), ("poseidon2", 3), ("keccak", 1), ("monolith", 4), ("poseidonbn128", 2)):
         t0 = time.perf_counter()
         (O.ref_merkle_fill if O.ref_available() else O.merkle_fill)(sample, w, ch, ht)
         res[name]["cpu_reference_leaf_elems_per_s"] = (1 << 14) * w / (time.perf_counter() - t0)

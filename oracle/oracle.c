@@ -8,7 +8,7 @@
  * Parity is pinned (tests/test_oracle.py) against
  *   - the known-answer vectors of zeknox's own tests (native/tests/tests.cu
  *     Poseidon :279-292, Poseidon2 :409-428, Keccak :164-173, Monolith
- *     :201-203; Go Merkle caps
+ *     :201-203, Poseidon-BN128 :492-501; Go Merkle caps
  *     wrappers/go/lib/lib_test.go:194-213), committed in tests/golden/, and
  *   - outputs of zeknox's own C++ CPU Merkle path compiled from its sources
  *     (oracle/build_ref.sh -> oracle/_ref/), committed as fixtures.
@@ -239,8 +239,144 @@ void orc_monolith_permute(u64 st[12]) {
     }
 }
 
+/* --------------------------------------------------------- Poseidon-BN128 */
+/* poseidon/poseidon_bn128.cu:111-193 with the field of element_bn128.cu:
+ * circomlib's Poseidon over the BN254 scalar field r, t = 5, 8 full and 60
+ * partial rounds in the optimised form (constants C, M, P, S in Montgomery
+ * form, R = 2^256).  The 12 Goldilocks lanes (canonical) become 4 field
+ * elements x_i = in[3i+2] + in[3i+1] 2^64 + in[3i] 2^128; the state is
+ * (0, x_0..x_3); after the permutation lane i of the output is limb 2 - (i mod 3)
+ * of state element i / 3, reduced mod p once. */
+static const u64 BN_R[4] = {0x43e1f593f0000001ull, 0x2833e84879b97091ull, 0xb85045b68181585dull,
+                            0x30644e72e131a029ull};
+static const u64 BN_NINV = 0xc2e1f593efffffffull;  /* -r^-1 mod 2^64 */
+static const u64 BN_R2[4] = {0x1bb8e645ae216da7ull, 0x53fe3ab1e35c59e3ull, 0x8c49833d53bb8085ull,
+                             0x0216d0b17f4e44a5ull};  /* 2^512 mod r */
+static int bn_geq(const u64 a[4], const u64 b[4]) {
+    for (int i = 3; i >= 0; i--)
+        if (a[i] != b[i]) return a[i] > b[i];
+    return 1;
+}
+static void bn_sub_r(u64 a[4]) {
+    u64 borrow = 0;
+    for (int i = 0; i < 4; i++) {
+        u128 d = (u128)a[i] - BN_R[i] - borrow;
+        a[i] = (u64)d;
+        borrow = (u64)(d >> 64) ? 1 : 0;
+    }
+}
+static void bn_add(u64 z[4], const u64 x[4], const u64 y[4]) {
+    u64 c = 0, t[4];
+    for (int i = 0; i < 4; i++) {
+        u128 s = (u128)x[i] + y[i] + c;
+        t[i] = (u64)s;
+        c = (u64)(s >> 64);
+    }
+    if (bn_geq(t, BN_R)) bn_sub_r(t);  /* x, y < r < 2^254: no carry out */
+    memcpy(z, t, 32);
+}
+/* Montgomery product x y / 2^256 mod r (CIOS), fully reduced. */
+static void bn_mul(u64 z[4], const u64 x[4], const u64 y[4]) {
+    u64 t[6] = {0};
+    for (int i = 0; i < 4; i++) {
+        u64 c = 0;
+        for (int j = 0; j < 4; j++) {
+            u128 v = (u128)x[j] * y[i] + t[j] + c;
+            t[j] = (u64)v;
+            c = (u64)(v >> 64);
+        }
+        u128 v = (u128)t[4] + c;
+        t[4] = (u64)v;
+        t[5] = (u64)(v >> 64);
+        u64 m = t[0] * BN_NINV;
+        v = (u128)m * BN_R[0] + t[0];
+        c = (u64)(v >> 64);
+        for (int j = 1; j < 4; j++) {
+            v = (u128)m * BN_R[j] + t[j] + c;
+            t[j - 1] = (u64)v;
+            c = (u64)(v >> 64);
+        }
+        v = (u128)t[4] + c;
+        t[3] = (u64)v;
+        t[4] = t[5] + (u64)(v >> 64);
+    }
+    u64 out[4] = {t[0], t[1], t[2], t[3]};
+    if (t[4] || bn_geq(out, BN_R)) bn_sub_r(out);
+    memcpy(z, out, 32);
+}
+static void bn_exp5(u64 x[4]) {
+    u64 x2[4], x4[4];
+    bn_mul(x2, x, x);
+    bn_mul(x4, x2, x2);
+    bn_mul(x, x4, x);
+}
+/* new[i] = sum_j m[j][i] state[j] */
+static void bn_mix(u64 st[5][4], const u64 *m) {
+    u64 out[5][4];
+    for (int i = 0; i < 5; i++) {
+        u64 acc[4] = {0}, prod[4];
+        for (int j = 0; j < 5; j++) {
+            bn_mul(prod, m + 4 * (5 * j + i), st[j]);
+            bn_add(acc, acc, prod);
+        }
+        memcpy(out[i], acc, 32);
+    }
+    memcpy(st, out, sizeof(out));
+}
+static void bn_ark(u64 st[5][4], int it) {
+    for (int i = 0; i < 5; i++) bn_add(st[i], st[i], ZK_BN128_C + 4 * (it + i));
+}
+void orc_poseidon_bn128_permute(u64 lanes[12]) {
+    u64 st[5][4];
+    memset(st, 0, sizeof(st));
+    for (int i = 0; i < 4; i++) {
+        u64 x[4] = {lanes[3 * i + 2] % P, lanes[3 * i + 1] % P, lanes[3 * i] % P, 0};
+        bn_mul(st[i + 1], x, BN_R2);  /* to Montgomery form */
+    }
+    bn_ark(st, 0);
+    for (int r = 0; r < 3; r++) {
+        for (int i = 0; i < 5; i++) bn_exp5(st[i]);
+        bn_ark(st, 5 * (r + 1));
+        bn_mix(st, ZK_BN128_M);
+    }
+    for (int i = 0; i < 5; i++) bn_exp5(st[i]);
+    bn_ark(st, 20);
+    bn_mix(st, ZK_BN128_P);
+    for (int r = 0; r < 60; r++) {
+        bn_exp5(st[0]);
+        bn_add(st[0], st[0], ZK_BN128_C + 4 * (25 + r));
+        const u64 *sp = ZK_BN128_S + 4 * 9 * r;
+        u64 acc[4] = {0}, prod[4];
+        for (int j = 0; j < 5; j++) {
+            bn_mul(prod, sp + 4 * j, st[j]);
+            bn_add(acc, acc, prod);
+        }
+        for (int k = 1; k < 5; k++) {
+            bn_mul(prod, st[0], sp + 4 * (5 + k - 1));
+            bn_add(st[k], st[k], prod);
+        }
+        memcpy(st[0], acc, 32);
+    }
+    for (int r = 0; r < 3; r++) {
+        for (int i = 0; i < 5; i++) bn_exp5(st[i]);
+        bn_ark(st, 85 + 5 * r);
+        bn_mix(st, ZK_BN128_M);
+    }
+    for (int i = 0; i < 5; i++) bn_exp5(st[i]);
+    bn_mix(st, ZK_BN128_M);
+    const u64 one[4] = {1, 0, 0, 0};
+    for (int i = 0; i < 4; i++) {
+        u64 v[4];
+        bn_mul(v, st[i], one);  /* out of Montgomery form */
+        for (int k = 0; k < 3; k++) {
+            u64 w = v[2 - k];
+            lanes[3 * i + k] = w >= P ? w - P : w;
+        }
+    }
+}
+
 /* ---------------------------------------------------------------- hashers */
-enum { H_POSEIDON = 0, H_KECCAK = 1, H_POSEIDON2 = 3, H_MONOLITH = 4 };
+enum { H_POSEIDON = 0, H_KECCAK = 1, H_POSEIDON_BN128 = 2, H_POSEIDON2 = 3, H_MONOLITH = 4 };
 
 /* Sponge of poseidon/poseidon_permutation.cuh:226-276 (GPU) and
  * poseidon_permutation.hpp:84-139 (CPU): width 12, rate 8, overwrite mode.
@@ -293,6 +429,7 @@ int orc_hash_one(int ht, const u64 *in, u64 n, u64 out[4]) {
     case H_POSEIDON: sponge_hash_one(orc_poseidon_permute, in, n, out); return 0;
     case H_POSEIDON2: sponge_hash_one(orc_poseidon2_permute, in, n, out); return 0;
     case H_MONOLITH: sponge_hash_one(orc_monolith_permute, in, n, out); return 0;
+    case H_POSEIDON_BN128: sponge_hash_one(orc_poseidon_bn128_permute, in, n, out); return 0;
     case H_KECCAK: keccak_hash_one(in, n, out); return 0;
     default: return -1;
     }
@@ -302,6 +439,7 @@ int orc_hash_two(int ht, const u64 *l, const u64 *r, u64 out[4]) {
     case H_POSEIDON: sponge_hash_two(orc_poseidon_permute, l, r, out); return 0;
     case H_POSEIDON2: sponge_hash_two(orc_poseidon2_permute, l, r, out); return 0;
     case H_MONOLITH: sponge_hash_two(orc_monolith_permute, l, r, out); return 0;
+    case H_POSEIDON_BN128: sponge_hash_two(orc_poseidon_bn128_permute, l, r, out); return 0;
     case H_KECCAK: keccak_hash_two(l, r, out); return 0;
     default: return -1;
     }
@@ -319,7 +457,7 @@ int orc_hash_two(int ht, const u64 *l, const u64 *r, u64 out[4]) {
  *    H2(node 0, node 1). */
 int orc_merkle_fill(u64 *digests, u64 *cap, const u64 *leaves, u64 n_digests, u64 n_caps,
                     u64 n_leaves, u64 leaf_size, u64 cap_height, int ht) {
-    if (ht != H_POSEIDON && ht != H_POSEIDON2 && ht != H_KECCAK && ht != H_MONOLITH) return -1;
+    if (ht < H_POSEIDON || ht > H_MONOLITH) return -1;
     if (n_caps == n_leaves) {
 #pragma omp parallel for schedule(static)
         for (long long i = 0; i < (long long)n_leaves; i++)

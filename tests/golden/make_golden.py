@@ -6,7 +6,8 @@ kat.json
     line each one comes from (parsed from those files, not typed in):
     Poseidon hash_one sizes 1..9 (native/tests/tests.cu:279-292), Poseidon2
     Fibonacci input (tests.cu:409-428), Keccak sizes 1..6 (tests.cu:164-173),
-    Monolith hash_one of 0..11 (tests.cu:201-203) and the Go Merkle caps
+    Monolith hash_one of 0..11 (tests.cu:201-203), Poseidon-BN128 hash_one
+    (tests.cu:492-501) and the Go Merkle caps
     (wrappers/go/lib/lib_test.go:194-213).
 
 merkle_ref_cpu.npz
@@ -36,7 +37,7 @@ MERKLE_SHAPES = [
     (32, 4, 1), (32, 3, 1), (128, 8, 3), (512, 13, 2), (256, 135, 4),
 ]
 HASHES = {"poseidon": O.HASH_POSEIDON, "poseidon2": O.HASH_POSEIDON2, "keccak": O.HASH_KECCAK,
-          "monolith": O.HASH_MONOLITH}
+          "monolith": O.HASH_MONOLITH, "poseidonbn128": O.HASH_POSEIDON_BN128}
 
 
 def _u64s(txt):
@@ -68,6 +69,10 @@ def parse_kats(zk: Path) -> dict:
     mono_in = _u64s(block(tests, 203, 203).split("=", 1)[1])
     mono_exp = _u64s(block(tests, 204, 204).split("=", 1)[1])
     kat["monolith_hash_one"] = {"source": "native/tests/tests.cu:201-204", "input": mono_in, "expected": mono_exp}
+    # Poseidon-BN128: input at tests.cu:494-499, expected digest at :501.
+    bn_in = _u64s(block(tests, 494, 499).split("=", 1)[1])
+    bn_exp = _u64s(block(tests, 501, 501).split("=", 1)[1])
+    kat["poseidon_bn128_hash_one"] = {"source": "native/tests/tests.cu:492-501", "input": bn_in, "expected": bn_exp}
     # Go caps: leaf at lib_test.go:195, three (nLeaves, nCaps, expHash) cases.
     gl = _u64s(block(gotest, 195, 195).split("{", 1)[1])
     cases = []
@@ -79,6 +84,7 @@ def parse_kats(zk: Path) -> dict:
     kat["go_merkle_caps"] = {"source": "wrappers/go/lib/lib_test.go:194-213", "leaf": gl, "cases": cases}
     assert len(cases) == 3 and len(exp) >= 10 and len(kexp) == 7 and len(p2) == 4
     assert len(mono_in) == 12 and len(mono_exp) == 4
+    assert len(bn_in) == 12 and len(bn_exp) == 4
     return kat
 
 

@@ -9,7 +9,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-HASHES = {"poseidon": 0, "poseidon2": 3, "keccak": 1, "monolith": 4}
+HASHES = {"poseidon": 0, "poseidon2": 3, "keccak": 1, "monolith": 4, "poseidonbn128": 2}
 
 
 @pytest.fixture(scope="module")
@@ -67,6 +67,9 @@ def test_hash_one_kats(zk, golden):
     mk = golden["kat"]["monolith_hash_one"]
     _, cap = gpu_tree(zk, np.array(mk["input"], dtype=np.uint64), 12, 0, 4)
     assert cap.tolist() == mk["expected"]
+    bk = golden["kat"]["poseidon_bn128_hash_one"]
+    _, cap = gpu_tree(zk, np.array(bk["input"], dtype=np.uint64), 12, 0, 2)
+    assert cap.tolist() == bk["expected"]
 
 
 def test_go_merkle_caps(zk, golden):
@@ -95,7 +98,7 @@ def test_vs_reference_cpu_fixtures(zk, oracle, golden):
             assert np.array_equal(d, golden["merkle"][key + "_digests"]), key
 
 
-@pytest.mark.parametrize("ht", [0, 3, 1, 4])
+@pytest.mark.parametrize("ht", [0, 3, 1, 4, 2])
 @pytest.mark.parametrize("nl,ls,ch", [(4096, 135, 4), (2048, 8, 0), (1024, 17, 10), (8192, 5, 3), (64, 200, 5),
                                      (1 << 16, 24, 0), (1 << 16, 9, 6), (1 << 15, 12, 12)])
 def test_vs_oracle(zk, oracle, ht, nl, ls, ch):
@@ -145,14 +148,14 @@ def test_invalid_sizes_and_unsupported_hash(zk, oracle):
     dd, dc = _dev(np.zeros(120 * 4, dtype=np.uint64)), _dev(np.full(4 * 4, 7, dtype=np.uint64))
     with pytest.raises(zk.ZeknoxError):  # digests size inconsistent with leaves / cap
         zk.fill_digests_buf_linear_gpu_with_gpu_ptr(dd.data_ptr(), dc.data_ptr(), dl.data_ptr(), 100, 4, 64, 9, 2, 0)
-    for ht in (2, 5):  # PoseidonBN128 (not built) / no such hasher: nothing written
+    for ht in (5, 6):  # no such hasher: nothing written
         with pytest.raises(zk.ZeknoxError):
             zk.fill_digests_buf_linear_gpu_with_gpu_ptr(dd.data_ptr(), dc.data_ptr(), dl.data_ptr(), 120, 4, 64, 9, 2,
                                                         ht)
     assert (_host(dc) == 7).all()
 
 
-@pytest.mark.parametrize("ht", [0, 3, 1, 4])
+@pytest.mark.parametrize("ht", [0, 3, 1, 4, 2])
 def test_full_size_tree_properties(zk, oracle, ht):
     """2^20 leaves x 135 (the hash-sweep shape): every cap entry, 4096 random
     internal nodes and 512 random leaf digests re-derived with the oracle."""
@@ -183,7 +186,7 @@ def test_full_size_tree_properties(zk, oracle, ht):
 
 
 # ---------------------------------------------- zeknox's own sm_100a build
-@pytest.mark.parametrize("ht", [0, 3, 1, 4])
+@pytest.mark.parametrize("ht", [0, 3, 1, 4, 2])
 def test_vs_zeknox_sm100_build(zk, oracle, ht):
     from oracle.oracle import HERE
 

@@ -14,6 +14,11 @@ parameters):
   circulant matrix, read from ``native/monolith/monolith.cu``
   (``MONOLITH_ROUND_CONSTANTS`` at monolith.cu:11, ``MONOLITH_MAT_12`` at :103);
   only the matrix's first row is kept, after checking that it is circulant.
+* Poseidon-BN128 (circomlib Poseidon over the BN254 scalar field, t = 5, in
+  its optimised form): round constants C[100], sparse matrices S[540], MDS
+  M[5][5] and the pre-sparse matrix P[5][5], each a 4 x 64-bit Montgomery
+  value, read from ``native/poseidon/poseidon_bn128_constants.h`` (:16, :119,
+  :662, :700).
 * Keccak-f[1600]: the 24 iota constants and the rho rotation offsets are not
   copied; they are computed here from the FIPS 202 definitions (the rc(t) LFSR
   with polynomial x^8+x^6+x^5+x^4+1, and offsets (t+1)(t+2)/2 along the
@@ -91,6 +96,7 @@ def main() -> None:
     pos = (src / "poseidon/poseidon.hpp").read_text()
     p2 = (src / "poseidon2/poseidon2.cu").read_text()
     mono = (src / "monolith/monolith.cu").read_text()
+    bn = (src / "poseidon/poseidon_bn128_constants.h").read_text()
 
     rc = _table(pos, "ALL_ROUND_CONSTANTS")
     circ = _table(pos, "MDS_MATRIX_CIRC")
@@ -103,6 +109,9 @@ def main() -> None:
     mono_mat = _table(mono, "MONOLITH_MAT_12")
     assert len(mono_rc) == 84 and len(mono_mat) == 144
     mono_row = mono_mat[:12]
+    bn_c, bn_s = _table(bn, "CONST u64 C"), _table(bn, "CONST u64 S")
+    bn_m, bn_p = _table(bn, "CONST u64 M"), _table(bn, "CONST u64 P")
+    assert len(bn_c) == 400 and len(bn_s) == 2160 and len(bn_m) == 100 and len(bn_p) == 100
     assert all(mono_mat[12 * r + c] == mono_row[(c - r) % 12] for r in range(12) for c in range(12)), "not circulant"
     kc = keccak_round_constants()
     rho = keccak_rho_offsets()
@@ -144,6 +153,12 @@ def main() -> None:
         arr("ZK_MONOLITH_RC", mono_rc),
         "// Monolith concrete layer: circulant, row r column c uses ZK_MONOLITH_MDS_ROW[(c - r) mod 12].",
         arr("ZK_MONOLITH_MDS_ROW", mono_row),
+        "// Poseidon-BN128 (t = 5), Montgomery form, 4 little-endian 64-bit limbs per value:",
+        "// round constants C[100], sparse matrices S[540] (9 per partial round), M[5][5], P[5][5].",
+        arr("ZK_BN128_C", bn_c),
+        arr("ZK_BN128_S", bn_s),
+        arr("ZK_BN128_M", bn_m),
+        arr("ZK_BN128_P", bn_p),
         "// Keccak-f[1600] iota constants (24 rounds).",
         arr("ZK_KECCAK_RC", kc),
         "// Rho rotation offsets per lane (index x + 5y).",

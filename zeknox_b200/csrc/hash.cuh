@@ -9,6 +9,7 @@
 //   Keccak     native/keccak/keccak.cu:42-135 (rate 136 B, 0x01 .. 0x80 pad,
 //              digest word 3 masked to its low byte)
 //   Monolith   native/monolith/monolith.cu:117-233
+//   Poseidon-BN128  native/poseidon/poseidon_bn128.cu:111-193
 //   sponge     native/poseidon/poseidon_permutation.cuh:226-276 (rate 8,
 //              overwrite mode, n <= 4 copies and zero-pads)
 #pragma once
@@ -450,8 +451,176 @@ __device__ __forceinline__ void monolith_permute(uint64_t s[12], const MonolithT
     }
 }
 
+// ---------------------------------------------------- Poseidon-BN128
+// circomlib's Poseidon over the BN254 scalar field r, t = 5, 8 full and 60
+// partial rounds in the optimised form (native/poseidon/poseidon_bn128.cu:
+// 111-193), field arithmetic of element_bn128.cu: Montgomery form with
+// R = 2^256, four 64-bit limbs, every result fully reduced.  The 12
+// Goldilocks lanes become 4 field elements x_i = lane[3i+2] + lane[3i+1] 2^64
+// + lane[3i] 2^128; the state is (0, x_0, .., x_3).  Output lane 3i + k is
+// limb 2 - k of state element i, reduced mod p once.
+struct BnTab {
+    uint64_t c[100][4];  // round constants
+    uint64_t s[540][4];  // sparse partial-round matrices, 9 values per round
+    uint64_t m[25][4];   // MDS, m[5 j + i] multiplies state j into lane i
+    uint64_t p[25][4];   // pre-sparse matrix (same indexing)
+};
+constexpr BnTab make_bn_tab() {
+    BnTab t{};
+    constexpr uint64_t c[400] = {ZK_BN128_C_LIST};
+    constexpr uint64_t sp[2160] = {ZK_BN128_S_LIST};
+    constexpr uint64_t m[100] = {ZK_BN128_M_LIST};
+    constexpr uint64_t pm[100] = {ZK_BN128_P_LIST};
+    for (int i = 0; i < 400; i++) t.c[i / 4][i % 4] = c[i];
+    for (int i = 0; i < 2160; i++) t.s[i / 4][i % 4] = sp[i];
+    for (int i = 0; i < 100; i++) t.m[i / 4][i % 4] = m[i];
+    for (int i = 0; i < 100; i++) t.p[i / 4][i % 4] = pm[i];
+    return t;
+}
+__constant__ BnTab c_bn128 = make_bn_tab();
+__device__ BnTab g_bn128 = make_bn_tab();
+
+struct Fr {
+    uint64_t v[4];
+};
+__host__ __device__ constexpr uint64_t bn_r(int i) {  // the modulus r, little-endian limbs
+    constexpr uint64_t r[4] = {0x43e1f593f0000001ull, 0x2833e84879b97091ull, 0xb85045b68181585dull,
+                               0x30644e72e131a029ull};
+    return r[i];
+}
+constexpr uint64_t kBnNinv = 0xc2e1f593efffffffull;  // -r^-1 mod 2^64
+constexpr uint64_t kBnR2[4] = {0x1bb8e645ae216da7ull, 0x53fe3ab1e35c59e3ull, 0x8c49833d53bb8085ull,
+                               0x0216d0b17f4e44a5ull};  // 2^512 mod r
+
+// t - r if t >= r (t < 2r), limb-wise with borrows.
+__device__ __forceinline__ void bn_reduce_once(uint64_t t[4], uint64_t top) {
+    uint64_t d[4];
+    uint64_t borrow = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const uint64_t ri = bn_r(i) + borrow;
+        const uint64_t b1 = ri < borrow ? 1 : 0;  // r_i + 1 overflowed
+        d[i] = t[i] - ri;
+        borrow = (t[i] < ri ? 1 : 0) | b1;
+    }
+    const bool ge = top || !borrow;
+#pragma unroll
+    for (int i = 0; i < 4; i++) t[i] = ge ? d[i] : t[i];
+}
+__device__ __forceinline__ Fr bn_add(const Fr &x, const Fr &y) {
+    Fr z;
+    uint64_t c = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const uint64_t s1 = x.v[i] + y.v[i];
+        const uint64_t c1 = s1 < x.v[i] ? 1 : 0;
+        const uint64_t s2 = s1 + c;
+        c = c1 | (s2 < s1 ? 1 : 0);
+        z.v[i] = s2;
+    }
+    bn_reduce_once(z.v, c);
+    return z;
+}
+// Montgomery product x y / 2^256 mod r (CIOS over 64-bit limbs).
+__device__ __forceinline__ Fr bn_mul(const Fr &x, const Fr &y) {
+    uint64_t t[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        uint64_t c = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const unsigned __int128 v = (unsigned __int128)x.v[j] * y.v[i] + t[j] + c;
+            t[j] = (uint64_t)v;
+            c = (uint64_t)(v >> 64);
+        }
+        unsigned __int128 v = (unsigned __int128)t[4] + c;
+        t[4] = (uint64_t)v;
+        t[5] = (uint64_t)(v >> 64);
+        const uint64_t m = t[0] * kBnNinv;
+        v = (unsigned __int128)m * bn_r(0) + t[0];
+        c = (uint64_t)(v >> 64);
+#pragma unroll
+        for (int j = 1; j < 4; j++) {
+            v = (unsigned __int128)m * bn_r(j) + t[j] + c;
+            t[j - 1] = (uint64_t)v;
+            c = (uint64_t)(v >> 64);
+        }
+        v = (unsigned __int128)t[4] + c;
+        t[3] = (uint64_t)v;
+        t[4] = t[5] + (uint64_t)(v >> 64);
+    }
+    Fr z{{t[0], t[1], t[2], t[3]}};
+    bn_reduce_once(z.v, t[4]);
+    return z;
+}
+__device__ __forceinline__ Fr bn_load(const uint64_t (&a)[4]) { return Fr{{a[0], a[1], a[2], a[3]}}; }
+__device__ __forceinline__ Fr bn_exp5(const Fr &x) {
+    const Fr x2 = bn_mul(x, x);
+    const Fr x4 = bn_mul(x2, x2);
+    return bn_mul(x4, x);
+}
+// st <- M^T st (new_i = sum_j m[5 j + i] st_j)
+__device__ __forceinline__ void bn_mix(Fr st[5], const uint64_t (*m)[4]) {
+    Fr out[5];
+#pragma unroll 1
+    for (int i = 0; i < 5; i++) {
+        Fr acc = bn_mul(bn_load(m[i]), st[0]);
+#pragma unroll
+        for (int j = 1; j < 5; j++) acc = bn_add(acc, bn_mul(bn_load(m[5 * j + i]), st[j]));
+        out[i] = acc;
+    }
+#pragma unroll
+    for (int i = 0; i < 5; i++) st[i] = out[i];
+}
+
+__device__ __forceinline__ void poseidon_bn128_permute(uint64_t s[12], const BnTab &tab = c_bn128) {
+    Fr st[5];
+    st[0] = Fr{{0, 0, 0, 0}};
+    const Fr r2{{kBnR2[0], kBnR2[1], kBnR2[2], kBnR2[3]}};
+#pragma unroll
+    for (int i = 0; i < 4; i++) st[i + 1] = bn_mul(Fr{{s[3 * i + 2], s[3 * i + 1], s[3 * i], 0}}, r2);
+#pragma unroll
+    for (int i = 0; i < 5; i++) st[i] = bn_add(st[i], bn_load(tab.c[i]));
+#pragma unroll 1
+    for (int r = 0; r < 4; r++) {  // full rounds 1-4: S-box, constants, M (P for the 4th)
+#pragma unroll
+        for (int i = 0; i < 5; i++) st[i] = bn_exp5(st[i]);
+#pragma unroll
+        for (int i = 0; i < 5; i++) st[i] = bn_add(st[i], bn_load(tab.c[5 * (r + 1) + i]));
+        bn_mix(st, r < 3 ? tab.m : tab.p);
+    }
+#pragma unroll 1
+    for (int r = 0; r < 60; r++) {  // partial rounds with the sparse matrices
+        st[0] = bn_add(bn_exp5(st[0]), bn_load(tab.c[25 + r]));
+        const uint64_t (*sp)[4] = tab.s + 9 * r;
+        Fr acc = bn_mul(bn_load(sp[0]), st[0]);
+#pragma unroll
+        for (int j = 1; j < 5; j++) acc = bn_add(acc, bn_mul(bn_load(sp[j]), st[j]));
+#pragma unroll
+        for (int k = 1; k < 5; k++) st[k] = bn_add(st[k], bn_mul(st[0], bn_load(sp[4 + k])));
+        st[0] = acc;
+    }
+#pragma unroll 1
+    for (int r = 0; r < 4; r++) {  // full rounds 5-8 (no constants in the last)
+#pragma unroll
+        for (int i = 0; i < 5; i++) st[i] = bn_exp5(st[i]);
+        if (r < 3) {
+#pragma unroll
+            for (int i = 0; i < 5; i++) st[i] = bn_add(st[i], bn_load(tab.c[85 + 5 * r + i]));
+        }
+        bn_mix(st, tab.m);
+    }
+    const Fr one{{1, 0, 0, 0}};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const Fr v = bn_mul(st[i], one);  // out of Montgomery form
+#pragma unroll
+        for (int k = 0; k < 3; k++) s[3 * i + k] = gl_canon(v.v[2 - k]);
+    }
+}
+
 // ------------------------------------------------------------ hashers
-enum : int { kPoseidon = 0, kKeccak = 1, kPoseidon2 = 3, kMonolith = 4 };
+enum : int { kPoseidon = 0, kKeccak = 1, kPoseidonBN128 = 2, kPoseidon2 = 3, kMonolith = 4 };
 
 // Leaf elements are reduced mod p when read (a no-op for canonical inputs).
 template <int H, int W = 4>
@@ -506,6 +675,7 @@ __device__ __forceinline__ void hash_one(const uint64_t *__restrict__ in, uint32
             }
             if constexpr (H == kPoseidon) poseidon_permute<W>(s);
             else if constexpr (H == kMonolith) monolith_permute(s);
+            else if constexpr (H == kPoseidonBN128) poseidon_bn128_permute(s);
             else poseidon2_permute<W>(s);
         }
         out[0] = gl_canon(s[0]);
@@ -533,11 +703,16 @@ template <>
 struct TabOf<kMonolith> {
     using type = MonolithTab;
 };
+template <>
+struct TabOf<kPoseidonBN128> {
+    using type = BnTab;
+};
 template <int H>
 __device__ __forceinline__ const typename TabOf<H>::type &const_tab() {
     if constexpr (H == kPoseidon) return c_poseidon;
     else if constexpr (H == kPoseidon2) return c_poseidon2;
     else if constexpr (H == kMonolith) return c_monolith;
+    else if constexpr (H == kPoseidonBN128) return c_bn128;
     else return c_keccak_tab;
 }
 
@@ -547,6 +722,7 @@ __device__ __forceinline__ const typename TabOf<H>::type *global_tab() {
     if constexpr (H == kPoseidon) return &g_poseidon;
     else if constexpr (H == kPoseidon2) return &g_poseidon2;
     else if constexpr (H == kMonolith) return &g_monolith;
+    else if constexpr (H == kPoseidonBN128) return &g_bn128;
     else return nullptr;
 }
 
@@ -583,6 +759,7 @@ __device__ __forceinline__ void hash_two(const uint64_t *l, const uint64_t *r, u
         }
         if constexpr (H == kPoseidon) poseidon_permute<W>(s, tab);
         else if constexpr (H == kMonolith) monolith_permute(s, tab);
+        else if constexpr (H == kPoseidonBN128) poseidon_bn128_permute(s, tab);
         else poseidon2_permute<W>(s, tab);
         out[0] = gl_canon(s[0]);
         out[1] = gl_canon(s[1]);

@@ -245,7 +245,7 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
 }  // namespace
 
 bool merkle_hash_supported(uint64_t ht) {
-    return ht == kPoseidon || ht == kPoseidon2 || ht == kKeccak || ht == kMonolith;
+    return ht == kPoseidon || ht == kPoseidon2 || ht == kKeccak || ht == kMonolith || ht == kPoseidonBN128;
 }
 
 void merkle_validate(const MerkleJob &j) {
@@ -268,6 +268,7 @@ void merkle_run(const MerkleJob &j, cudaStream_t st) {
     case kPoseidon2: merkle_run_t<kPoseidon2>(j, st); break;
     case kKeccak: merkle_run_t<kKeccak>(j, st); break;
     case kMonolith: merkle_run_t<kMonolith>(j, st); break;
+    case kPoseidonBN128: merkle_run_t<kPoseidonBN128>(j, st); break;
     default: break;
     }
 }
