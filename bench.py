@@ -220,7 +220,7 @@ def main() -> None:
     ap.add_argument("--jobs", type=int, default=0)
     ap.add_argument("--streams", type=int, default=4)
     ap.add_argument("--budget-gb", type=int, default=120)
-    ap.add_argument("--rates", type=float, nargs="*", default=[0.5, 1.0, 1.25])
+    ap.add_argument("--rates", type=float, nargs="*", default=[0.25, 0.5, 0.75, 1.0, 1.25])
     args = ap.parse_args()
     if args.workload != "commit" and args.impl == "ours":
         {"merkle": run_merkle_only, "sweep": run_sweep, "batched": run_batched, "served": run_served}[args.workload](args)
