@@ -157,6 +157,17 @@ ZK_EXTERN RustError zk_lde_leaves_async(void *d_leaves, const void *d_coeffs, ui
 ZK_EXTERN RustError zk_commit_async(const void *d_coeffs, uint32_t lg_n, uint32_t rate_bits, uint32_t batches,
                                     uint32_t cap_height, uint32_t hash_type, void *d_leaves, void *d_digests,
                                     void *d_cap, void *stream);
+/* Opening proofs on a resident forest (zeknox's linear layout, the output of
+ * zk_merkle_async / fill_digests_buf_linear_gpu_with_gpu_ptr): for each of the
+ * n_queries leaf indices in d_indices, its leaf row (leaf_size words, into
+ * d_out_leaves) and the log2(n_leaves >> cap_height) sibling digests from the
+ * leaf level up to the level below the cap (Plonky2's MerkleProof order), into
+ * d_out_siblings (n_queries x depth x 4 words).  The path of leaf i ends at cap
+ * entry i >> (log2(n_leaves) - cap_height).  Stream-ordered, device buffers;
+ * a query index >= n_leaves gets all-ones words. */
+ZK_EXTERN RustError zk_merkle_open_async(const void *d_leaves, const void *d_digests, uint64_t n_leaves,
+                                         uint64_t leaf_size, uint64_t cap_height, const uint64_t *d_indices,
+                                         uint64_t n_queries, void *d_out_leaves, void *d_out_siblings, void *stream);
 ZK_EXTERN RustError zk_merkle_async(void *d_digests, void *d_cap, const void *d_leaves, uint64_t n_digests,
                                     uint64_t n_caps, uint64_t n_leaves, uint64_t leaf_size, uint64_t cap_height,
                                     uint64_t hash_type, void *stream);

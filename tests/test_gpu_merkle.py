@@ -208,3 +208,49 @@ def test_vs_zeknox_sm100_build(zk, oracle, ht):
     ref_d, ref_c = _host(dd), _host(dc)
     d, c = gpu_tree(zk, leaves, ls, ch, ht)
     assert np.array_equal(c, ref_c) and np.array_equal(d, ref_d)
+
+
+# ------------------------------------------------- opening proofs (resident tree)
+def _verify_path(oracle, ht, row, sib, index, cap, cap_height, n_leaves):
+    """Plonky2's MerkleProof check: hash the leaf, fold the siblings bottom-up
+    (the running digest is the left input when its index bit is 0), compare
+    with the cap entry the path ends at."""
+    cur = oracle.hash_one(ht, row)
+    for lvl, s in enumerate(sib):
+        cur = oracle.hash_two(ht, cur, s) if ((index >> lvl) & 1) == 0 else oracle.hash_two(ht, s, cur)
+    depth = (n_leaves >> cap_height).bit_length() - 1
+    return np.array_equal(cur, cap[index >> depth])
+
+
+@pytest.mark.parametrize("ht,nl,ls,ch", [(0, 1 << 12, 135, 4), (3, 1 << 11, 24, 0), (1, 1 << 10, 7, 3),
+                                         (4, 1 << 9, 16, 2), (2, 256, 9, 1), (0, 64, 12, 6)])
+def test_opening_paths_verify_against_cap(zk, oracle, ht, nl, ls, ch):
+    import torch
+
+    leaves = oracle.field_elems(500 + ht * 13 + nl, nl * ls)
+    lt = _dev(leaves).view(nl, ls)
+    digests, cap = zk.merkle_tree(lt, ch, ht)
+    rng = np.random.default_rng(ht + nl)
+    q = rng.integers(0, nl, size=64)
+    rows, sib = zk.merkle_open(lt, digests, ch, torch.from_numpy(q))
+    torch.cuda.synchronize()
+    rows, sib, capn = rows.cpu().numpy(), sib.cpu().numpy(), cap.cpu().numpy()
+    depth = (nl >> ch).bit_length() - 1
+    assert sib.shape == (64, depth, 4)
+    for k, i in enumerate(q):
+        assert np.array_equal(rows[k], leaves[i * ls:(i + 1) * ls])
+        assert _verify_path(oracle, ht, rows[k], sib[k], int(i), capn, ch, nl), (ht, int(i))
+
+
+def test_opening_out_of_range_index(zk, oracle):
+    import torch
+
+    nl, ls, ch = 128, 9, 2
+    leaves = oracle.field_elems(77, nl * ls)
+    lt = _dev(leaves).view(nl, ls)
+    digests, _ = zk.merkle_tree(lt, ch, 0)
+    rows, sib = zk.merkle_open(lt, digests, ch, torch.tensor([5, nl, 127]))
+    torch.cuda.synchronize()
+    rows, sib = rows.cpu().numpy(), sib.cpu().numpy()
+    assert (rows[1] == np.uint64(2**64 - 1)).all() and (sib[1] == np.uint64(2**64 - 1)).all()
+    assert np.array_equal(rows[0], leaves[5 * ls:6 * ls]) and np.array_equal(rows[2], leaves[127 * ls:128 * ls])

@@ -230,3 +230,22 @@ def merkle_tree(leaves, cap_height: int, hash_type: int = HashPoseidon, digests=
     capi.check(capi.LIB.zk_merkle_async(digests.data_ptr(), cap.data_ptr(), leaves.data_ptr(), n_digests, n_caps,
                                         n_leaves, w, cap_height, hash_type, _stream_ptr(stream)))
     return digests, cap
+
+
+def merkle_open(leaves, digests, cap_height: int, indices, stream=None):
+    """Opening proofs on a resident forest: for each leaf index, its leaf row and
+    the sibling digests from the leaf level up to the level below the cap
+    (Plonky2's MerkleProof order).  -> (rows (Q, w), siblings (Q, depth, 4)) CUDA
+    tensors; the path of leaf i ends at cap entry i >> (log2(L) - cap_height)."""
+    import torch
+
+    assert leaves.dtype == torch.uint64 and leaves.is_cuda and leaves.is_contiguous() and leaves.dim() == 2
+    n_leaves, w = leaves.shape
+    idx = indices.to(device=leaves.device, dtype=torch.int64).contiguous().view(torch.uint64)
+    q = idx.numel()
+    depth = (n_leaves >> cap_height).bit_length() - 1
+    rows = torch.empty((q, w), dtype=torch.uint64, device=leaves.device)
+    sib = torch.empty((q, depth, 4), dtype=torch.uint64, device=leaves.device)
+    capi.check(capi.LIB.zk_merkle_open_async(leaves.data_ptr(), digests.data_ptr(), n_leaves, w, cap_height,
+                                             idx.data_ptr(), q, rows.data_ptr(), sib.data_ptr(), _stream_ptr(stream)))
+    return rows, sib

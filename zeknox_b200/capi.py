@@ -111,6 +111,7 @@ def _load() -> ctypes.CDLL:
         "zk_lde_async": (RustError, [vp, vp, u32, u32, u32, u32, u32, vp]),
         "zk_transpose_rev_async": (RustError, [vp, vp, u32, u32, vp]),
         "zk_merkle_async": (RustError, [vp, vp, vp, u64, u64, u64, u64, u64, u64, vp]),
+        "zk_merkle_open_async": (RustError, [vp, vp, u64, u64, u64, vp, u64, vp, vp, vp]),
         "zk_lde_noalloc": (RustError, [vp, vp, u32, u32, u32, u32, u32, vp]),
         "zk_lde_leaves_async": (RustError, [vp, vp, u32, u32, u32, vp]),
         "zk_commit_async": (RustError, [vp, u32, u32, u32, u32, u32, vp, vp, vp, vp]),

@@ -514,6 +514,17 @@ extern "C" RustError zk_transpose_rev_async(void *d_output, const void *d_input,
     });
 }
 
+extern "C" RustError zk_merkle_open_async(const void *d_leaves, const void *d_digests, uint64_t n_leaves,
+                                         uint64_t leaf_size, uint64_t cap_height, const uint64_t *d_indices,
+                                         uint64_t n_queries, void *d_out_leaves, void *d_out_siblings,
+                                         void *stream) {
+    return guarded([&] {
+        merkle_open((const uint64_t *)d_leaves, (const uint64_t *)d_digests, n_leaves, leaf_size, cap_height,
+                    d_indices, n_queries, (uint64_t *)d_out_leaves, (uint64_t *)d_out_siblings,
+                    (cudaStream_t)stream);
+    });
+}
+
 extern "C" RustError zk_merkle_async(void *d_digests, void *d_cap, const void *d_leaves, uint64_t n_digests,
                                     uint64_t n_caps, uint64_t n_leaves, uint64_t leaf_size, uint64_t cap_height,
                                     uint64_t hash_type, void *stream) {

@@ -244,6 +244,68 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
 
 }  // namespace
 
+namespace {
+
+// Opening proofs on a resident forest.  Leaf rows: one thread per (query, word).
+__global__ void merkle_open_leaves(const uint64_t *__restrict__ leaves, uint64_t n_leaves, uint64_t leaf_size,
+                                   const uint64_t *__restrict__ idx, uint64_t n_queries, uint64_t *__restrict__ out) {
+    const uint64_t total = n_queries * leaf_size;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t q = t / leaf_size, k = t - q * leaf_size, i = idx[q];
+        out[t] = i < n_leaves ? leaves[i * leaf_size + k] : ~0ull;
+    }
+}
+
+// Siblings: one thread per (query, level).  Level lvl of leaf j (in its
+// subtree) is the level of width w = Ls >> lvl at offset w - 2; the sibling of
+// node j >> lvl is node (j >> lvl) ^ 1.
+__global__ void merkle_open_paths(const uint64_t *__restrict__ digests, uint64_t n_leaves, uint32_t lg_ls, uint64_t ds,
+                                  const uint64_t *__restrict__ idx, uint64_t n_queries, uint64_t *__restrict__ out) {
+    const uint64_t total = n_queries * lg_ls;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t q = t / lg_ls, lvl = t - q * lg_ls, i = idx[q];
+        uint64_t *o = out + 4 * t;
+        if (i >= n_leaves) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) o[k] = ~0ull;
+            continue;
+        }
+        const uint64_t ls = 1ull << lg_ls, s = i >> lg_ls, j = i & (ls - 1);
+        const uint64_t w = ls >> lvl;
+        const uint64_t *d = digests + 4 * (s * ds + (w - 2) + ((j >> lvl) ^ 1));
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = d[k];
+    }
+}
+
+unsigned grid_for(uint64_t n) {
+    const uint64_t b = (n + 255) / 256;
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(b, 148ull * 32));
+}
+
+}  // namespace
+
+void merkle_open(const uint64_t *leaves, const uint64_t *digests, uint64_t n_leaves, uint64_t leaf_size,
+                 uint64_t cap_height, const uint64_t *idx, uint64_t n_queries, uint64_t *out_leaves,
+                 uint64_t *out_siblings, cudaStream_t st) {
+    require(cap_height < 64 && n_leaves >= (1ull << cap_height) && n_leaves % (1ull << cap_height) == 0,
+            "n_leaves must be a multiple of 2^cap_height");
+    const uint64_t ls = n_leaves >> cap_height;
+    require((ls & (ls - 1)) == 0, "leaves per subtree must be a power of two");
+    require(leaf_size > 0, "leaf_size out of range");
+    if (n_queries == 0) return;
+    require(idx && leaves && out_leaves, "null buffer");
+    const uint32_t lg_ls = (uint32_t)__builtin_ctzll(ls);
+    merkle_open_leaves<<<grid_for(n_queries * leaf_size), 256, 0, st>>>(leaves, n_leaves, leaf_size, idx, n_queries,
+                                                                       out_leaves);
+    ZK_CHECK_LAUNCH();
+    if (lg_ls == 0) return;
+    require(digests && out_siblings, "null buffer");
+    merkle_open_paths<<<grid_for(n_queries * lg_ls), 256, 0, st>>>(digests, n_leaves, lg_ls, 2 * ls - 2, idx, n_queries,
+                                                                   out_siblings);
+    ZK_CHECK_LAUNCH();
+}
+
 bool merkle_hash_supported(uint64_t ht) {
     return ht == kPoseidon || ht == kPoseidon2 || ht == kKeccak || ht == kMonolith || ht == kPoseidonBN128;
 }

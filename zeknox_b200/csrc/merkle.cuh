@@ -17,5 +17,9 @@ struct MerkleJob {
 bool merkle_hash_supported(uint64_t hash_type);
 void merkle_validate(const MerkleJob &job);  // throws zk::Error
 void merkle_run(const MerkleJob &job, cudaStream_t s);
+// Leaf rows and sibling paths of n_queries leaves (all pointers on the device).
+void merkle_open(const uint64_t *leaves, const uint64_t *digests, uint64_t n_leaves, uint64_t leaf_size,
+                 uint64_t cap_height, const uint64_t *idx, uint64_t n_queries, uint64_t *out_leaves,
+                 uint64_t *out_siblings, cudaStream_t s);
 
 }  // namespace zk
