@@ -26,7 +26,7 @@ def _dev(a):
 
 
 @pytest.mark.parametrize("lg_n,rate,b", [(4, 1, 3), (9, 3, 17), (10, 2, 135), (12, 3, 33), (15, 3, 135),
-                                         (17, 2, 5), (18, 3, 7), (8, 1, 200)])
+                                         (17, 2, 5), (18, 3, 7), (8, 1, 200), (20, 3, 3), (21, 3, 2)])
 def test_lde_leaves_equals_lde_then_transpose(zk, oracle, lg_n, rate, b):
     import torch
 

@@ -373,7 +373,8 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
 __global__ void __launch_bounds__(kNttThreads) ntt_last_pass_leaves(PassArgs a) {
     extern __shared__ uint64_t smem[];
     const uint32_t l = a.l, L = 1u << l;
-    const uint32_t P = 1u << a.lg_t, tp = P + 1;
+    // Row pitch as pass_smem sizes it (one polynomial: no padding column).
+    const uint32_t P = 1u << a.lg_t, tp = P > 1 ? P + 1 : 1;
     uint64_t *tw = smem;
     uint64_t *sm = smem + L;
     for (uint32_t j = threadIdx.x; j < L; j += blockDim.x) tw[j] = __ldg(a.line_roots + (j << (kLineLgMax - l)));
@@ -613,7 +614,7 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
                 a.kind = 3;
                 a.lg_s = 0;
                 a.lg_pre = lg - a.l;
-                a.lg_t = a.l <= 9 ? 3 : 12 - a.l;
+                a.lg_t = a.l <= 9 ? 3 : 12 - std::min<uint32_t>(a.l, 12);
                 a.src = scr;
                 a.src_poly_stride = N;
                 a.dst = j.dst + b0;
