@@ -464,8 +464,21 @@ struct Plan {
     uint32_t l[3];
 };
 
-Plan make_plan(uint32_t lg) {
+// to_leaves: the last pass writes each leaf row in runs of 8 polynomials only
+// while its lines are at most 2^9 points (shared memory); with two passes the
+// runs shrink to 4 words at 2^20-2^21, 2 at 2^22-2^23 and 1 at 2^24.  Measured
+// (B200, LDE to leaves): three passes win from 2^22 on (2^22 x 48 polys 7.5 ->
+// 6.7 ms, 2^23 x 24 8.4 -> 6.8 ms, 2^24 x 12 12.0 -> 8.7 ms) and lose below
+// (2^20 x 64 1.7 -> 2.4 ms), so transforms of 2^22..2^24 points take three.
+Plan make_plan(uint32_t lg, bool to_leaves = false) {
     Plan p{};
+    if (to_leaves && lg >= 22 && lg <= 24) {
+        p.passes = 3;
+        p.l[0] = (lg + 2) / 3;
+        p.l[1] = (lg - p.l[0] + 1) / 2;
+        p.l[2] = lg - p.l[0] - p.l[1];
+        return p;
+    }
     if (lg <= 12) {
         p.passes = 1;
         p.l[0] = lg;
@@ -526,7 +539,7 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
     DeviceCtx &ctx = device_ctx(current_device());
     const PowTable &rt = root_table(ctx, lg, j.inverse);
     const uint64_t *lr = line_roots(ctx, j.inverse);
-    const Plan plan = make_plan(lg);
+    const Plan plan = make_plan(lg, j.to_leaves);
     const uint64_t N = 1ull << lg;
 
     PassArgs base{};
