@@ -49,6 +49,24 @@ NCU_TRAFFIC = {
 }
 
 
+def max_over_ranks(values, dist, device) -> list:
+    """Each timing is the maximum over the ranks (one all-reduce; identity
+    for a single process).  `device` holds the reduction tensor: the rank's
+    GPU under NCCL, the CPU under gloo."""
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def replica_throughput(world: int, units_per_step: int, steps: int, ms_max: float) -> float:
+    """Whole-job units per second of `world` independent replicas, each doing
+    `units_per_step` per step, timed by the slowest rank."""
+    return world * units_per_step * steps / (ms_max * 1e-3)
+
+
 def set_workload(polys=135, lg_n=15, rate=3, cap_h=4, hash_name="poseidon", rot=4):
     """Workload of one step; the defaults are the plain single-job commit
     (135 x 2^15 coefficients, rate 3, Poseidon, cap height 4)."""
@@ -342,13 +360,10 @@ def main() -> None:
     e2e_input = (args.steps - 1) % N_ROT
 
     # ---- max over ranks ----
-    ms_t = torch.tensor([ms, e2e_s, ms_plain], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max, e2e_max, ms_plain = float(ms_t[0]), float(ms_t[1]), float(ms_t[2])
+    ms_max, e2e_max, ms_plain = max_over_ranks([ms, e2e_s, ms_plain], dist, dev)
 
     if rank == 0:
-        value = world * B * N * args.steps / (ms_max * 1e-3)
+        value = replica_throughput(world, B * N, args.steps, ms_max)
         e2e_val = world * B * N * args.steps / e2e_max
         peaks = measured_peaks()
         hbm_peak = peaks.get("hbm_gbs")
