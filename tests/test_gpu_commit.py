@@ -158,3 +158,29 @@ def test_server_large_job_lane_is_fifo(zk, oracle, monkeypatch):
         for t, w in zip(tickets, want):
             assert np.array_equal(srv.wait(t)[0], w)
             srv.release(t)
+
+
+def test_commit_batch_graph_replays_bit_exact(zk, oracle):
+    """A batch captured into a CUDA graph reproduces the individual commits,
+    and commits new coefficients written into the same inputs on replay."""
+    import torch
+
+    jobs = _mixed_jobs(oracle, 10, 31)
+    items = []
+    for x, r, ch, ht in jobs:
+        d = _dev(x)
+        b, n = d.shape
+        items.append((d, r, ch, ht, zk.CommitBuffers(n << r, b, ch)))
+    g = zk.CommitGraph(items)
+    for round_ in range(2):
+        if round_:  # new values in the captured input buffers
+            for k, (d, r, ch, ht, o) in enumerate(items):
+                d.copy_(_dev(oracle.field_elems(900 + k, d.numel()).reshape(d.shape)))
+        g.replay()
+        torch.cuda.synchronize()
+        for d, r, ch, ht, o in items:
+            alone = zk.commit(d, r, ch, ht)
+            torch.cuda.synchronize()
+            assert torch.equal(alone.cap.view(torch.int64), o.cap.view(torch.int64))
+            assert torch.equal(alone.digests.view(torch.int64), o.digests.view(torch.int64))
+            assert torch.equal(alone.leaves.view(torch.int64), o.leaves.view(torch.int64))
