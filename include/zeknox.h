@@ -201,6 +201,17 @@ typedef struct {
  * job's outputs equal zk_commit_async's. */
 ZK_EXTERN RustError zk_commit_batch(const ZkCommitJob *jobs, uint32_t n_jobs, uint32_t n_streams, void *stream);
 
+/* Autotuner of the LDE -> leaves stage (commits, batches, the server): for
+ * one shape (2^lg_n coefficients, rate_bits, batches polynomials) it times
+ * every legal pass count (2 or 3) and polynomials-per-block of the leaves pass
+ * on scratch data and keeps the fastest for that size and batch-size class;
+ * later transforms of that class use it.  Outputs do not depend on the
+ * choice.  Synchronous: call outside stream capture.  *timed receives the
+ * number of candidates timed (0: already tuned, or a one-pass size).
+ * zk_autotune_reset forgets every choice. */
+ZK_EXTERN RustError zk_autotune_commit(uint32_t lg_n, uint32_t rate_bits, uint32_t batches, int32_t *timed);
+ZK_EXTERN RustError zk_autotune_reset(void);
+
 /* Commit server: jobs are submitted with host coefficients (kept valid by the
  * caller until the job completes), admitted onto n_slots concurrent streams
  * while leaves + digests + cap of resident trees plus coefficients + scratch of

@@ -184,3 +184,22 @@ def test_commit_batch_graph_replays_bit_exact(zk, oracle):
             assert torch.equal(alone.cap.view(torch.int64), o.cap.view(torch.int64))
             assert torch.equal(alone.digests.view(torch.int64), o.digests.view(torch.int64))
             assert torch.equal(alone.leaves.view(torch.int64), o.leaves.view(torch.int64))
+
+
+def test_autotuner_choices_keep_outputs_bit_exact(zk, oracle):
+    """Tuning the LDE -> leaves stage changes only how it runs: commits of the
+    tuned shapes equal the untuned ones, and a tuned shape is not re-timed."""
+    import torch
+
+    zk.autotune_reset()
+    for lg_n, rate, b in [(12, 3, 33), (15, 3, 135), (19, 3, 5), (21, 3, 2)]:
+        x = _dev(oracle.field_elems(4400 + lg_n, b << lg_n)).view(b, 1 << lg_n)
+        before = zk.commit(x, rate, 4, 0)
+        torch.cuda.synchronize()
+        assert zk.autotune(lg_n, rate, b) >= 1
+        assert zk.autotune(lg_n, rate, b) == 0
+        after = zk.commit(x, rate, 4, 0)
+        torch.cuda.synchronize()
+        assert torch.equal(before.leaves.view(torch.int64), after.leaves.view(torch.int64))
+        assert torch.equal(before.cap.view(torch.int64), after.cap.view(torch.int64))
+    zk.autotune_reset()

@@ -131,6 +131,20 @@ def commit_batch(items, n_streams: int = 4, stream=None):
                                         _stream_ptr(stream)))
 
 
+def autotune(lg_n: int, rate_bits: int, batches: int) -> int:
+    """Tune the LDE -> leaves stage for this shape (zk_autotune_commit); returns
+    the number of candidates timed (0: already tuned or nothing to choose)."""
+    import ctypes
+
+    n = ctypes.c_int32()
+    capi.check(capi.LIB.zk_autotune_commit(lg_n, rate_bits, batches, ctypes.byref(n)))
+    return n.value
+
+
+def autotune_reset():
+    capi.check(capi.LIB.zk_autotune_reset())
+
+
 class CommitGraph:
     """A batch of commits (commit_batch items) captured once into a CUDA graph.
 

@@ -120,6 +120,8 @@ def _load() -> ctypes.CDLL:
         "zk_server_submit": (RustError, [vp, vp, u32, u32, u32, u32, u32, ctypes.POINTER(u64)]),
         "zk_server_wait": (RustError, [vp, u64, vp, ctypes.POINTER(ctypes.c_double)]),
         "zk_server_wait_any": (RustError, [vp, u32, ctypes.POINTER(u64)]),
+        "zk_autotune_commit": (RustError, [u32, u32, u32, ctypes.POINTER(ctypes.c_int32)]),
+        "zk_autotune_reset": (RustError, []),
         "zk_server_result": (RustError, [vp, u64, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)]),
         "zk_server_release": (RustError, [vp, u64]),
         "zk_server_stats": (RustError, [vp, ctypes.POINTER(ZkServerStats)]),

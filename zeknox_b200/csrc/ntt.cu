@@ -20,6 +20,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <map>
+#include <mutex>
 
 #include "gl64.cuh"
 #include "ntt.cuh"
@@ -531,6 +533,49 @@ void launch_leaves_pass(const PassArgs &a, uint64_t groups, cudaStream_t s) {
 
 }  // namespace
 
+// ---- autotuning of the LDE -> leaves stage ----
+// Per (transform size, batch-size class): the number of passes (2 or 3) and
+// the polynomials per block of the leaves pass (2^lg_t), chosen by timing the
+// candidates on the device (ntt_autotune_leaves).  Untuned shapes use the
+// static choice of make_plan and 8 polynomials per block.
+struct LeavesChoice {
+    uint8_t passes = 0;  // 0: no entry
+    uint8_t lg_t = 0;
+};
+std::mutex g_tune_mu;
+std::map<uint64_t, LeavesChoice> g_tune;
+thread_local const LeavesChoice *t_tune_override = nullptr;  // set while the tuner times a candidate
+
+uint64_t tune_key(uint32_t lg, uint64_t batches) {
+    const uint64_t cls = 64 - __builtin_clzll(batches);  // batch-size class: bit length
+    return ((uint64_t)lg << 8) | cls;
+}
+
+LeavesChoice leaves_choice(uint32_t lg, uint64_t batches) {
+    if (t_tune_override) return *t_tune_override;
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune.find(tune_key(lg, batches));
+    return it == g_tune.end() ? LeavesChoice{} : it->second;
+}
+
+Plan plan_with_passes(uint32_t lg, int passes) {
+    Plan p{};
+    p.passes = passes;
+    if (passes == 2) {
+        p.l[0] = (lg + 1) / 2;
+        p.l[1] = lg - p.l[0];
+    } else {
+        p.l[0] = (lg + 2) / 3;
+        p.l[1] = (lg - p.l[0] + 1) / 2;
+        p.l[2] = lg - p.l[0] - p.l[1];
+    }
+    return p;
+}
+
+// Leaves-pass block of 2^lg_t polynomials over lines of 2^l points fits the
+// 160 KB of dynamic shared memory the pass launches with.
+bool leaves_fits(uint32_t l, uint32_t lg_t) { return pass_smem(l, lg_t) <= 160 * 1024; }
+
 // One batched transform of `batches` polynomials of 2^lg elements.
 void ntt_run(const NttJob &j, cudaStream_t s) {
     const uint32_t lg = j.lg;
@@ -539,7 +584,8 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
     DeviceCtx &ctx = device_ctx(current_device());
     const PowTable &rt = root_table(ctx, lg, j.inverse);
     const uint64_t *lr = line_roots(ctx, j.inverse);
-    const Plan plan = make_plan(lg, j.to_leaves);
+    const LeavesChoice tuned = j.to_leaves ? leaves_choice(lg, j.batches) : LeavesChoice{};
+    const Plan plan = tuned.passes ? plan_with_passes(lg, tuned.passes) : make_plan(lg, j.to_leaves);
     const uint64_t N = 1ull << lg;
 
     PassArgs base{};
@@ -628,6 +674,7 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
                 a.lg_s = 0;
                 a.lg_pre = lg - a.l;
                 a.lg_t = a.l <= 9 ? 3 : 12 - std::min<uint32_t>(a.l, 12);
+                if (tuned.passes && leaves_fits(a.l, tuned.lg_t)) a.lg_t = tuned.lg_t;
                 a.src = scr;
                 a.src_poly_stride = N;
                 a.dst = j.dst + b0;
@@ -778,6 +825,86 @@ void ntt_run_on_tables(const NttJob &j, const PowTable &roots, const uint64_t *l
             }
         }
     }
+}
+
+// Times every legal (passes, polynomials per block) pair of the LDE -> leaves
+// stage for this shape on scratch data (outputs do not depend on the choice)
+// and records the fastest.  Synchronous; call it outside stream capture.
+// Returns the number of candidates timed (0 if the shape was tuned already or
+// has one pass).
+int ntt_autotune_leaves(uint32_t lg_n, uint32_t rate_bits, uint64_t batches, cudaStream_t s) {
+    const uint32_t lg = lg_n + rate_bits;
+    require(lg >= 1 && lg <= 30 && batches >= 1, "invalid shape");
+    if (make_plan(lg).passes == 1) return 0;
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        if (g_tune.count(tune_key(lg, batches))) return 0;
+    }
+    DeviceCtx &ctx = device_ctx(current_device());
+    const uint64_t N = 1ull << lg, n = 1ull << lg_n;
+    // a representative batch: the class's own size, capped at ~1 GiB of leaves
+    const uint64_t bt = std::max<uint64_t>(1, std::min<uint64_t>(batches, (1ull << 27) / N));
+    Scratch in(bt * n * sizeof(uint64_t), s), out(bt * N * sizeof(uint64_t), s);
+    const uint64_t scr_elems = ntt_scratch_elems(lg, bt);
+    Scratch scr(scr_elems * sizeof(uint64_t), s);
+    ZK_CUDA(cudaMemsetAsync(in.p, 0, bt * n * sizeof(uint64_t), s));
+    NttJob j;
+    j.src = in.as<uint64_t>();
+    j.src_stride = n;
+    j.n_valid = n;
+    j.dst = out.as<uint64_t>();
+    j.batches = bt;
+    j.lg = lg;
+    j.pre_coset = &coset_table(ctx, lg, GROUP_GENERATOR, false);
+    j.to_leaves = true;
+    j.scratch = scr.as<uint64_t>();
+    j.scratch_elems = scr_elems;
+    cudaEvent_t e0, e1;
+    ZK_CUDA(cudaEventCreate(&e0));
+    ZK_CUDA(cudaEventCreate(&e1));
+    LeavesChoice best{};
+    float best_ms = 1e30f;
+    int timed = 0;
+    try {
+        for (int passes = 2; passes <= 3; passes++) {
+            if (passes == 2 && lg > 24) continue;
+            const Plan p = plan_with_passes(lg, passes);
+            const uint32_t l_last = p.l[passes - 1];
+            for (uint32_t lg_t = 2; lg_t <= 4; lg_t++) {
+                if (!leaves_fits(l_last, lg_t)) continue;
+                const LeavesChoice c{(uint8_t)passes, (uint8_t)lg_t};
+                t_tune_override = &c;
+                ntt_run(j, s);  // warm-up
+                ZK_CUDA(cudaEventRecord(e0, s));
+                ntt_run(j, s);
+                ntt_run(j, s);
+                ZK_CUDA(cudaEventRecord(e1, s));
+                t_tune_override = nullptr;
+                ZK_CUDA(cudaEventSynchronize(e1));
+                float ms = 0;
+                ZK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                timed++;
+                if (ms < best_ms) best_ms = ms, best = c;
+            }
+        }
+    } catch (...) {
+        t_tune_override = nullptr;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (best.passes) {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        g_tune[tune_key(lg, batches)] = best;
+    }
+    return timed;
+}
+
+void ntt_autotune_clear() {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune.clear();
 }
 
 }  // namespace zk

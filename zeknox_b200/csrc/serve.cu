@@ -201,6 +201,24 @@ extern "C" RustError zk_commit_batch(const ZkCommitJob *jobs, uint32_t n_jobs, u
     });
 }
 
+// ------------------------------------------------------------- autotuner
+
+extern "C" RustError zk_autotune_commit(uint32_t lg_n, uint32_t rate_bits, uint32_t batches, int32_t *timed) {
+    return guard([&] {
+        require(lg_n >= 1 && rate_bits >= 1 && lg_n + rate_bits <= 30 && batches >= 1, "invalid shape");
+        const int dev = current_device();
+        DeviceCtx &ctx = device_ctx(dev);
+        root_table(ctx, lg_n + rate_bits, false);
+        line_roots(ctx, false);
+        const int n = ntt_autotune_leaves(lg_n, rate_bits, batches, ctx.stream);
+        if (timed) *timed = n;
+    });
+}
+
+extern "C" RustError zk_autotune_reset(void) {
+    return guard([&] { ntt_autotune_clear(); });
+}
+
 // ------------------------------------------------------------------ server
 
 struct ZkServer {
