@@ -505,6 +505,9 @@ def run_sweep(args):
         ops = perms * OPS_PER_PERM.get(ht, 0)
         res[name] = {"ms": ms, "perm_per_s": perms / (ms * 1e-3), "leaf_elems_per_s": nl * w / (ms * 1e-3),
                      "int32_frac": ops / (ms * 1e-3) / peak if peak and ht in OPS_PER_PERM else None}
+    if args.no_cpu_baseline:
+        print(json.dumps(res), flush=True)
+        return
     # zeknox's CPU path on a 2^14-leaf sample of the same shape
     from oracle import oracle as O
 
