@@ -233,7 +233,7 @@ def main() -> None:
     ap.add_argument("--rate-bits", type=int, default=3)
     ap.add_argument("--cap-height", type=int, default=4)
     ap.add_argument("--hash", default="poseidon", choices=sorted(HASH_NAMES))
-    ap.add_argument("--workload", default="commit", choices=["commit", "merkle", "sweep", "batched", "served"],
+    ap.add_argument("--workload", default="commit", choices=["commit", "merkle", "sweep", "batched", "served", "fri"],
                     help="commit (default, the bench line); the others print their own JSON summary")
     ap.add_argument("--jobs", type=int, default=0)
     ap.add_argument("--streams", type=int, default=4)
@@ -241,7 +241,8 @@ def main() -> None:
     ap.add_argument("--rates", type=float, nargs="*", default=[0.25, 0.5, 0.75, 1.0, 1.25])
     args = ap.parse_args()
     if args.workload != "commit" and args.impl == "ours":
-        {"merkle": run_merkle_only, "sweep": run_sweep, "batched": run_batched, "served": run_served}[args.workload](args)
+        {"merkle": run_merkle_only, "sweep": run_sweep, "batched": run_batched, "served": run_served,
+         "fri": run_fri}[args.workload](args)
         return
     set_workload(args.polys, args.lg_n, args.rate_bits, args.cap_height, args.hash)
     if args.impl == "reference":
@@ -517,6 +518,74 @@ def run_sweep(args):
         t0 = time.perf_counter()
         (O.ref_merkle_fill if O.ref_available() else O.merkle_fill)(sample, w, ch, ht)
         res[name]["cpu_reference_leaf_elems_per_s"] = (1 << 14) * w / (time.perf_counter() - t0)
+    print(json.dumps(res), flush=True)
+
+
+def run_fri(args):
+    """FRI commit phase over a resident GF(p^2) polynomial of 2^15 coefficients at
+    rate 3 (2^18 points, the evaluation domain of the default commit), arity 16
+    three times, cap height 4, Poseidon; final polynomial of 8 coefficients.
+    `ms_with_transcript`: the phase as a prover runs it, a host round trip per
+    round for the Fiat-Shamir challenge; `ms_device`: the same kernels with the
+    challenges fixed in advance (device time only)."""
+    import torch
+
+    import zeknox_b200 as zk
+
+    lg_n, rate, arities, ch = 15, 3, [4, 4, 4], 4
+    n = 1 << lg_n
+    coeffs = _device_pool(torch, 2 * n, 0x5EED0006).view(2, n)
+    P = zk.P
+
+    def challenge(i, cap):
+        return (int(cap.reshape(-1)[0]) % P, int(cap.reshape(-1)[1]) % P)
+
+    for _ in range(args.warmup):
+        com = zk.fri_commit(coeffs, rate, arities, ch, challenge)
+    betas = [r.beta for r in com.rounds]
+    torch.cuda.synchronize()
+    reps = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        zk.fri_commit(coeffs, rate, arities, ch, challenge)
+    torch.cuda.synchronize()
+    ms_t = (time.perf_counter() - t0) * 1e3 / reps
+
+    # Device-only: the same launches with the challenges known in advance.
+    bufs = []
+    cur_n, shift = n, 7
+    for ab in arities:
+        N = cur_n << rate
+        leaves = torch.empty((N, 2), dtype=torch.uint64, device="cuda")
+        nd, nc = zk.merkle_sizes(N >> ab, ch)
+        bufs.append((leaves, torch.empty((max(nd, 1), 4), dtype=torch.uint64, device="cuda"),
+                     torch.empty((nc, 4), dtype=torch.uint64, device="cuda"),
+                     torch.empty((2, cur_n >> ab), dtype=torch.uint64, device="cuda"), shift, ab))
+        cur_n >>= ab
+        shift = pow(shift, 1 << ab, P)
+
+    def device_phase():
+        cur = coeffs
+        for (lv, d, c, nxt, sh, ab), beta in zip(bufs, betas):
+            zk.lde_leaves_coset(cur, rate, sh, out=lv)
+            zk.merkle_tree(lv.view(-1, 2 << ab), ch, 0, d, c)
+            zk.fri_fold(cur, ab, beta, out=nxt)
+            cur = nxt
+
+    device_phase()
+    final_dev = bufs[-1][3].clone()
+    ms_d = _ev_ms(torch, device_phase, reps)
+    res = {"workload": "fri commit phase: 2^15 GF(p^2) coefficients, rate 3, arity 16 x 3, cap_height 4, poseidon",
+           "ms_with_transcript": ms_t, "ms_device": ms_d, "points_per_s": (n << rate) / (ms_d * 1e-3),
+           "final_poly_equal": bool(torch.equal(final_dev, com.final_poly))}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        host = coeffs.cpu().numpy()
+        t0 = time.perf_counter()
+        _, fin = O.fri_commit(host, rate, arities, ch, challenge)
+        res["cpu_port_ms"] = (time.perf_counter() - t0) * 1e3
+        res["cpu_port_final_equal"] = bool(np.array_equal(fin, com.final_poly.cpu().numpy()))
     print(json.dumps(res), flush=True)
 
 

@@ -152,6 +152,21 @@ ZK_EXTERN RustError zk_transpose_rev_async(void *d_output, const void *d_input, 
  * intermediate LDE matrix. */
 ZK_EXTERN RustError zk_lde_leaves_async(void *d_leaves, const void *d_coeffs, uint32_t lg_n, uint32_t rate_bits,
                                         uint32_t batches, void *stream);
+/* zk_lde_leaves_async on the coset coset_gen * <w_N> instead of the installed
+ * one (the shifted cosets of FRI rounds: s_(i+1) = s_i^arity). */
+ZK_EXTERN RustError zk_lde_leaves_coset_async(void *d_leaves, const void *d_coeffs, uint32_t lg_n,
+                                              uint32_t rate_bits, uint32_t batches, uint64_t coset_gen,
+                                              void *stream);
+/* One FRI folding step over GF(p^2) = GF(p)[X]/(X^2 - 7) (no counterpart in
+ * zeknox; the step of the Plonky2 prover that consumes its commitments):
+ * d_out[j] = sum_(t < 2^arity_bits) beta^t * d_in[j * 2^arity_bits + t] for
+ * j < n_in >> arity_bits, beta = beta0 + beta1 X.  d_out is in the split
+ * layout (real parts, then the n_in >> arity_bits X parts); d_in is split
+ * (2 rows of n_in) or, with in_interleaved, n_in (real, X) pairs (16-byte
+ * aligned).  n_in a power of two, 1 <= arity_bits <= 6, canonical beta.  The
+ * next round's leaves are zk_lde_leaves_coset_async(batches = 2) of d_out. */
+ZK_EXTERN RustError zk_fri_fold_async(void *d_out, const void *d_in, uint64_t n_in, uint32_t arity_bits,
+                                      uint64_t beta0, uint64_t beta1, uint32_t in_interleaved, void *stream);
 /* One commit: zk_lde_leaves_async then the Merkle forest over those leaves
  * (digests 2*(N - 2^cap_height) x 4, cap 2^cap_height x 4, N = 2^(lg_n+rate_bits)). */
 ZK_EXTERN RustError zk_commit_async(const void *d_coeffs, uint32_t lg_n, uint32_t rate_bits, uint32_t batches,

@@ -581,3 +581,32 @@ void orc_transpose_rev(u64 *out, const u64 *in, unsigned lg_n, unsigned batches)
         for (u64 b = 0; b < batches; b++) out[r * batches + b] = in[b * n + k];
     }
 }
+
+/* -------------------------------------------------------------------- FRI */
+/* One folding step of the FRI commit phase over GF(p^2) = GF(p)[X]/(X^2 - 7),
+ * the quadratic extension of Goldilocks (W = 7).  The FRI prover that consumes
+ * zeknox's commitments is Plonky2's (okx/plonky2, rev 9a917ba2, the git
+ * dependency of wrappers/rust/Cargo.toml:43-44, not present here): each round
+ * reduces the coefficient vector by `arity`, coefficient j of the result being
+ * sum_t beta^t c[j*arity + t] ("reduce_with_powers").  Restated by Horner's
+ * rule from the highest power down.  Split layout in and out: row 0 real
+ * parts, row 1 X parts.  Parity against Plonky2 is unpinned (no copy of it). */
+static void ext_mul(u64 a0, u64 a1, u64 b0, u64 b1, u64 *c0, u64 *c1) {
+    u64 r0 = orc_add(orc_mul(a0, b0), orc_mul(7, orc_mul(a1, b1)));
+    u64 r1 = orc_add(orc_mul(a0, b1), orc_mul(a1, b0));
+    *c0 = r0;
+    *c1 = r1;
+}
+void orc_fri_fold(u64 *out, const u64 *in, u64 n_in, unsigned arity_bits, u64 b0, u64 b1) {
+    u64 a = 1ull << arity_bits, n_out = n_in >> arity_bits;
+    for (u64 j = 0; j < n_out; j++) {
+        u64 r0 = 0, r1 = 0;
+        for (u64 t = a; t-- > 0;) {
+            ext_mul(r0, r1, b0, b1, &r0, &r1);
+            r0 = orc_add(r0, in[j * a + t]);
+            r1 = orc_add(r1, in[n_in + j * a + t]);
+        }
+        out[j] = r0;
+        out[n_out + j] = r1;
+    }
+}

@@ -177,3 +177,54 @@ def test_transpose_rev_semantics(oracle):
     for k in range(1 << lg):
         r = int(format(k, f"0{lg}b")[::-1], 2)
         assert out[r].tolist() == m[:, k].tolist()
+
+
+# ---------------------------------------------------------------- FRI oracle
+def test_fri_fold_oracle_matches_definition(oracle):
+    """The C fold (Horner) against sum_t beta^t c[j a + t] in Python integers."""
+    n = 128
+    c = oracle.field_elems(77, 2 * n).reshape(2, n)
+    for ab, beta in [(1, (3, 5)), (3, (oracle.P - 1, 2)), (5, (0x1234567890ABCDEF, 0))]:
+        got = oracle.fri_fold(c, ab, beta)
+        a = 1 << ab
+        for j in range(n >> ab):
+            acc = (0, 0)
+            for t in range(a):
+                acc = oracle.ext_add(acc, oracle.ext_mul(oracle.ext_pow(beta, t), (int(c[0, j * a + t]), int(c[1, j * a + t]))))
+            assert (int(got[0, j]), int(got[1, j])) == acc
+
+
+def test_fri_extension_field_is_a_field(oracle):
+    """X^2 - 7 is irreducible over GF(p) (7 is a non-residue): x^(p^2-1) = 1 and
+    the inverse x^(p^2-2) really inverts."""
+    P = oracle.P
+    assert pow(7, (P - 1) // 2, P) == P - 1
+    for x in [(1, 1), (0, 1), (12345, 67890), (P - 1, 3)]:
+        assert oracle.ext_pow(x, P * P - 1) == (1, 0)
+        assert oracle.ext_mul(x, oracle.ext_pow(x, P * P - 2)) == (1, 0)
+
+
+@pytest.mark.parametrize("lg_n,rate,arities,cap_h", [(9, 2, [2, 3, 1], 1), (8, 3, [4], 2), (10, 1, [1, 1, 2, 3], 0)])
+def test_fri_oracle_rounds_fold_consistently(oracle, lg_n, rate, arities, cap_h):
+    """Every leaf row of a round, interpolated at beta as the FRI verifier does,
+    gives the next round's value at that position (the final polynomial after the
+    last round): the fold, the shifted-coset LDE and the bit-reversed leaf layout
+    agree with each other."""
+    P = oracle.P
+
+    def challenge(i, cap):
+        return (int(cap[0]) % P, int(cap[(1 + i) % cap.size]) % P)
+
+    c = oracle.field_elems(300 + lg_n, 2 << lg_n).reshape(2, -1)
+    rounds, final = oracle.fri_commit(c, rate, arities, cap_h, challenge)
+    assert final.shape == (2, (1 << lg_n) >> sum(arities))
+    for i, (r, ab) in enumerate(zip(rounds, arities)):
+        lg_N = (r["leaves"].size // 2).bit_length() - 1
+        m = r["leaves"].shape[0]
+        for j in sorted({0, 1, m // 3, m - 1}):
+            y, v = oracle.fri_fold_from_leaf(r["leaves"][j], j, lg_N, r["shift"], ab, r["beta"])
+            if i + 1 < len(rounds):
+                nxt = rounds[i + 1]["leaves"].reshape(-1, 2)[j]
+                assert v == (int(nxt[0]), int(nxt[1])), (i, j)
+            else:
+                assert v == oracle.ext_poly_eval(final, y), (i, j)

@@ -93,6 +93,21 @@ def lde_leaves(coeffs, rate_bits: int, out=None, stream=None):
     return out
 
 
+def lde_leaves_coset(coeffs, rate_bits: int, coset_gen: int, out=None, stream=None):
+    """lde_leaves on the coset coset_gen * <w_N> (zk_lde_leaves_coset_async)."""
+    import torch
+
+    assert coeffs.dtype == torch.uint64 and coeffs.is_cuda and coeffs.is_contiguous() and coeffs.dim() == 2
+    b, n = coeffs.shape
+    lg_n = n.bit_length() - 1
+    assert n == 1 << lg_n
+    if out is None:
+        out = torch.empty((n << rate_bits, b), dtype=torch.uint64, device=coeffs.device)
+    capi.check(capi.LIB.zk_lde_leaves_coset_async(out.data_ptr(), coeffs.data_ptr(), lg_n, rate_bits, b,
+                                                  coset_gen % P, _stream_ptr(stream)))
+    return out
+
+
 class CommitBuffers:
     """Device outputs of one commit: leaves (N, B), digests (2(N - 2^cap), 4), cap (2^cap, 4)."""
 
@@ -290,3 +305,84 @@ def merkle_open(leaves, digests, cap_height: int, indices, stream=None):
     capi.check(capi.LIB.zk_merkle_open_async(leaves.data_ptr(), digests.data_ptr(), n_leaves, w, cap_height,
                                              idx.data_ptr(), q, rows.data_ptr(), sib.data_ptr(), _stream_ptr(stream)))
     return rows, sib
+
+
+# ---------------------------------------------------------------- FRI
+def fri_fold(coeffs, arity_bits: int, beta, *, interleaved: bool = False, out=None, stream=None):
+    """One FRI folding step over GF(p^2) = GF(p)[X]/(X^2 - 7) (zk_fri_fold_async).
+
+    coeffs: (2, n) split (real parts, X parts) or, with `interleaved`, (n, 2)
+    (real, X) pairs, uint64 CUDA tensor.  -> (2, n >> arity_bits) split:
+    out[j] = sum_t beta^t coeffs[j 2^arity_bits + t], beta = (real, X part)."""
+    import torch
+
+    assert coeffs.dtype == torch.uint64 and coeffs.is_cuda and coeffs.is_contiguous() and coeffs.dim() == 2
+    n = coeffs.shape[0] if interleaved else coeffs.shape[1]
+    assert coeffs.shape == ((n, 2) if interleaved else (2, n))
+    if out is None:
+        out = torch.empty((2, n >> arity_bits), dtype=torch.uint64, device=coeffs.device)
+    capi.check(capi.LIB.zk_fri_fold_async(out.data_ptr(), coeffs.data_ptr(), n, arity_bits, int(beta[0]) % P,
+                                          int(beta[1]) % P, int(interleaved), _stream_ptr(stream)))
+    return out
+
+
+class FriRound:
+    """One committed FRI round: leaves (N_i >> arity_bits, 2^(arity_bits+1)) rows of
+    interleaved GF(p^2) evaluations in bit-reversed order, its Merkle forest, the
+    coset shift it was evaluated on and the challenge drawn from its cap."""
+
+    def __init__(self, leaves, digests, cap, arity_bits: int, shift: int):
+        self.leaves, self.digests, self.cap = leaves, digests, cap
+        self.arity_bits, self.shift = arity_bits, shift
+        self.beta = None
+
+
+class FriCommitment:
+    def __init__(self, rounds, final_poly, cap_height: int):
+        self.rounds, self.final_poly, self.cap_height = rounds, final_poly, cap_height
+
+
+def fri_commit(coeffs, rate_bits: int, arity_bits, cap_height: int, challenge, hash_type: int = HashPoseidon,
+               shift: int = 7, stream=None) -> FriCommitment:
+    """The FRI commit phase over a resident polynomial (Plonky2's prover loop).
+
+    coeffs: (2, n) split GF(p^2) coefficients on the device.  For each arity in
+    `arity_bits`: the values on the current coset (shift, then shift^arity, ...)
+    at rate `rate_bits` are written as leaves (zk_lde_leaves_coset_async,
+    2 polynomials) and committed (zk_merkle_async); `challenge(round, cap)`
+    (host callback, cap a (2^cap_height, 4) numpy array) returns beta; the
+    coefficients are folded by beta (zk_fri_fold_async).  The final folded
+    coefficients are returned on the device as `final_poly` (2, n / prod arity)."""
+    import torch
+
+    assert coeffs.dim() == 2 and coeffs.shape[0] == 2
+    cur = coeffs
+    rounds = []
+    for i, ab in enumerate(arity_bits):
+        n = cur.shape[1]
+        leaves = lde_leaves_coset(cur, rate_bits, shift, stream=stream)
+        view = leaves.view((n << rate_bits) >> ab, 2 << ab)
+        dig, cap = merkle_tree(view, cap_height, hash_type, stream=stream)
+        rnd = FriRound(view, dig, cap, ab, shift)
+        s = stream if stream is not None else torch.cuda.current_stream()
+        s.synchronize()
+        rnd.beta = challenge(i, cap.cpu().numpy())
+        rounds.append(rnd)
+        cur = fri_fold(cur, ab, rnd.beta, stream=stream)
+        shift = pow(shift, 1 << ab, P)
+    return FriCommitment(rounds, cur, cap_height)
+
+
+def fri_open(commitment: FriCommitment, indices, stream=None):
+    """Query openings of every FRI round for indices into the first round's
+    evaluation domain: round i opens leaf x >> (sum of the arity bits up to and
+    including round i), as the FRI query phase does.  -> list of (rows, siblings)."""
+    import torch
+
+    idx = torch.as_tensor(indices, dtype=torch.int64).cpu()
+    out = []
+    shift = 0
+    for rnd in commitment.rounds:
+        shift += rnd.arity_bits
+        out.append(merkle_open(rnd.leaves, rnd.digests, commitment.cap_height, idx >> shift, stream=stream))
+    return out

@@ -22,7 +22,7 @@ BUILD = PKG / "_build"
 SO = PKG / "libzeknox.so"
 AR = PKG / "libzeknox.a"
 PROBE = PKG / "libzkprobe.so"  # measurement aid for bench.py (INT32 issue rate), not the product ABI
-SOURCES = ["runtime.cu", "ntt.cu", "merkle.cu", "capi.cu", "noalloc.cu", "serve.cu"]
+SOURCES = ["runtime.cu", "ntt.cu", "merkle.cu", "fri.cu", "capi.cu", "noalloc.cu", "serve.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -114,6 +114,8 @@ def _load() -> ctypes.CDLL:
         "zk_merkle_open_async": (RustError, [vp, vp, u64, u64, u64, vp, u64, vp, vp, vp]),
         "zk_lde_noalloc": (RustError, [vp, vp, u32, u32, u32, u32, u32, vp]),
         "zk_lde_leaves_async": (RustError, [vp, vp, u32, u32, u32, vp]),
+        "zk_lde_leaves_coset_async": (RustError, [vp, vp, u32, u32, u32, u64, vp]),
+        "zk_fri_fold_async": (RustError, [vp, vp, u64, u32, u64, u64, u32, vp]),
         "zk_commit_async": (RustError, [vp, u32, u32, u32, u32, u32, vp, vp, vp, vp]),
         "zk_commit_batch": (RustError, [ctypes.POINTER(ZkCommitJob), u32, u32, vp]),
         "zk_server_create": (RustError, [ctypes.c_int32, u64, u32, ctypes.POINTER(vp)]),

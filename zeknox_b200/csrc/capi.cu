@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/zeknox.h"
+#include "fri.cuh"
 #include "merkle.cuh"
 #include "ntt.cuh"
 #include "runtime.cuh"
@@ -459,8 +460,9 @@ extern "C" RustError zk_lde_async(void *d_output, const void *d_input, uint32_t 
 
 namespace {
 // Forward coset LDE written in the leaf layout: leaves[rev(k)][b] = LDE_b[k].
+// `coset` null: the installed coset generator (7 unless init_coset changed it).
 void lde_leaves_device(DeviceCtx &ctx, uint64_t *d_leaves, const uint64_t *d_in, uint32_t lg_n, uint32_t rate_bits,
-                       uint64_t batches, cudaStream_t s) {
+                       uint64_t batches, cudaStream_t s, const PowTable *coset = nullptr) {
     const uint32_t lg = lg_n + rate_bits;
     require(lg_n >= 1 && rate_bits >= 1 && lg <= (uint32_t)kMaxLg, "invalid args");
     NttJob j;
@@ -470,7 +472,7 @@ void lde_leaves_device(DeviceCtx &ctx, uint64_t *d_leaves, const uint64_t *d_in,
     j.dst = d_leaves;
     j.batches = batches;
     j.lg = lg;
-    j.pre_coset = &coset_table(ctx, lg, GROUP_GENERATOR, false);
+    j.pre_coset = coset ? coset : &coset_table(ctx, lg, GROUP_GENERATOR, false);
     j.to_leaves = true;
     j.scratch_elems = ntt_scratch_elems(lg, batches);
     Scratch scr(j.scratch_elems * sizeof(uint64_t), s);
@@ -486,6 +488,29 @@ extern "C" RustError zk_lde_leaves_async(void *d_leaves, const void *d_coeffs, u
         require(d_leaves && d_coeffs, "null buffer");
         lde_leaves_device(ctx, (uint64_t *)d_leaves, (const uint64_t *)d_coeffs, lg_n, rate_bits, batches,
                           (cudaStream_t)stream);
+    });
+}
+
+extern "C" RustError zk_lde_leaves_coset_async(void *d_leaves, const void *d_coeffs, uint32_t lg_n,
+                                              uint32_t rate_bits, uint32_t batches, uint64_t coset_gen,
+                                              void *stream) {
+    return guarded([&] {
+        DeviceCtx &ctx = select((size_t)current_device());
+        require(d_leaves && d_coeffs, "null buffer");
+        require(coset_gen % P_HOST != 0, "coset generator must be non-zero");
+        require(lg_n >= 1 && rate_bits >= 1 && lg_n + rate_bits <= (uint32_t)kMaxLg, "invalid args");
+        const PowTable &t = shift_table(ctx, lg_n + rate_bits, coset_gen);
+        lde_leaves_device(ctx, (uint64_t *)d_leaves, (const uint64_t *)d_coeffs, lg_n, rate_bits, batches,
+                          (cudaStream_t)stream, &t);
+    });
+}
+
+extern "C" RustError zk_fri_fold_async(void *d_out, const void *d_in, uint64_t n_in, uint32_t arity_bits,
+                                      uint64_t beta0, uint64_t beta1, uint32_t in_interleaved, void *stream) {
+    return guarded([&] {
+        require(d_out && d_in, "null buffer");
+        fri_fold_run((uint64_t *)d_out, (const uint64_t *)d_in, n_in, arity_bits, beta0, beta1, in_interleaved != 0,
+                     (cudaStream_t)stream);
     });
 }
 

@@ -150,4 +150,14 @@ const PowTable &coset_table(DeviceCtx &c, unsigned lg, uint64_t gen, bool replac
     return t;
 }
 
+const PowTable &shift_table(DeviceCtx &c, unsigned bits, uint64_t base) {
+    require(bits <= (unsigned)kMaxLg, "shift table of 2^" + std::to_string(bits) + " powers out of range");
+    if (bits < 2) bits = 2;
+    base %= P_HOST;
+    std::lock_guard<std::mutex> g(c.mu);
+    PowTable &t = c.shifts[{base, bits}];  // std::map: references stay valid as it grows
+    if (!t.dev) t = make_pow_table(base, bits);
+    return t;
+}
+
 }  // namespace zk

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -85,6 +86,7 @@ struct DeviceCtx {
     uint64_t *line_roots[2] = {nullptr, nullptr};  // [dir] omega_4096^j, j < 4096
     PowTable roots[2][kMaxLg + 1];       // [dir][lg]: omega_{2^lg} powers
     PowTable coset;                      // coset_gen powers
+    std::map<std::pair<uint64_t, unsigned>, PowTable> shifts;  // other bases (base, bits), kept until exit
     std::mutex mu;
 };
 
@@ -98,6 +100,9 @@ const PowTable &root_table(DeviceCtx &c, unsigned lg, bool inverse);
 // Coset powers for at least 2^lg points.  A request with a different
 // generator replaces the table (init_coset semantics); a larger lg extends it.
 const PowTable &coset_table(DeviceCtx &c, unsigned lg, uint64_t gen, bool replace);
+// Powers of an arbitrary base for 2^bits exponents, built once per (base, bits)
+// and never replaced (the shifted cosets of FRI rounds use these).
+const PowTable &shift_table(DeviceCtx &c, unsigned bits, uint64_t base);
 
 // Stream-ordered scratch from the device's default memory pool.
 struct Scratch {
