@@ -358,6 +358,26 @@ def main() -> None:
     barrier()
     e2e_s = time.perf_counter() - t0
     cap_e2e = host_cap.numpy().copy()
+
+    # Where an end-to-end step's time goes (untimed pass, host clock per call;
+    # each call is synchronous or followed by a synchronize).
+    def e2e_phases(i: int):
+        t = [time.perf_counter()]
+        zk.lde_batch(local, lde_out.data_ptr(), pinned[i % N_ROT].data_ptr(), LG_N, cfg)
+        t.append(time.perf_counter())
+        zk.transpose_rev_batch(local, leaves.data_ptr(), lde_out.data_ptr(), LG, tcfg)
+        t.append(time.perf_counter())
+        zk.fill_digests_buf_linear_gpu_with_gpu_ptr(digests.data_ptr(), cap.data_ptr(), leaves.data_ptr(), nd, nc, N,
+                                                    B, CAP_H, HASH, local)
+        torch.cuda.synchronize()
+        t.append(time.perf_counter())
+        host_dig.copy_(digests, non_blocking=True)
+        host_cap.copy_(cap, non_blocking=True)
+        torch.cuda.synchronize()
+        t.append(time.perf_counter())
+        return np.diff(t) * 1e3
+
+    e2e_ph = np.median(np.array([e2e_phases(k) for k in range(5)]), axis=0)
     e2e_input = (args.steps - 1) % N_ROT
 
     # ---- max over ranks ----
@@ -410,7 +430,10 @@ def main() -> None:
             "e2e": {"value": e2e_val, "unit": "elems/s", "h2d_bytes_per_step": B * n * 8,
                     "d2h_bytes_per_step": (nd + nc) * 32,
                     "path": "compute_batched_lde (pinned host in) -> compute_transpose_rev -> "
-                            "fill_digests_buf_linear_gpu_with_gpu_ptr -> D2H digests+cap"},
+                            "fill_digests_buf_linear_gpu_with_gpu_ptr -> D2H digests+cap",
+                    "phases_ms": {"lde_with_h2d": float(e2e_ph[0]), "transpose": float(e2e_ph[1]),
+                                  "merkle": float(e2e_ph[2]), "d2h": float(e2e_ph[3]),
+                                  "note": "median of 5 untimed steps, host clock around each call"}},
             "gpu_launches": int(launches),
             "phases_ms": {"lde_to_leaves": t_lde, "merkle": t_mk},
             "plain_device_path": {"value": world * B * N * args.steps / (ms_plain * 1e-3), "unit": "elems/s",
