@@ -209,9 +209,9 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
         while (lg_top + 1 < map.lg_ls && lg_top < 5 && (j.n_caps << (lg_top + 1)) < kHexNodes) lg_top++;
         for (uint32_t lg_w = map.lg_ls - 1; lg_w > lg_top; lg_w--) {
             const uint64_t nodes = j.n_caps << lg_w;
-            if (nodes >= kHexNodes)
-                merkle_level<H, 4><<<blocks_for(nodes, kLeafThreads), kLeafThreads, 0, st>>>(j.digests, lg_w, j.n_caps,
-                                                                                             ds);
+            if (nodes >= kHexNodes)  // 12-lane S-box, as in the leaves (measured 15 us faster per tree of 2^18)
+                merkle_level<H, 12><<<blocks_for(nodes, kLeafThreads), kLeafThreads, 0, st>>>(j.digests, lg_w,
+                                                                                              j.n_caps, ds);
             else
                 merkle_level_hex<<<hex_blocks(nodes), kHexThreads, 0, st>>>(j.digests, lg_w, j.n_caps, ds);
             ZK_CHECK_LAUNCH();
