@@ -197,8 +197,10 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
         // latency- rather than issue-bound) in one launch.  Measured per
         // level: 16384 nodes 46 us six-threaded vs 40 us one-threaded (issue
         // bound: six threads do twice the instructions of one); 4096 nodes
-        // 20 us vs 40 us.
-        constexpr uint64_t kHexLeaves = 1 << 15, kHexNodes = 1 << 14;
+        // 20 us vs 40 us.  Whole trees of 135-word leaves, six-threaded vs
+        // one-threaded leaves: 8192 leaves 0.48 vs 0.65 ms, 16384 leaves 0.80
+        // vs 0.68 ms, 32768 leaves 1.43 vs 0.87 ms.
+        constexpr uint64_t kHexLeaves = 1 << 13, kHexNodes = 1 << 14;
         if (j.n_leaves <= kHexLeaves)
             merkle_leaves_hex<<<hex_blocks(j.n_leaves), kHexThreads, 0, st>>>(j.leaves, j.n_leaves, w, j.digests, map);
         else
