@@ -100,7 +100,8 @@ def test_vs_reference_cpu_fixtures(zk, oracle, golden):
 
 @pytest.mark.parametrize("ht", [0, 3, 1, 4, 2])
 @pytest.mark.parametrize("nl,ls,ch", [(4096, 135, 4), (2048, 8, 0), (1024, 17, 10), (8192, 5, 3), (64, 200, 5),
-                                     (1 << 16, 24, 0), (1 << 16, 9, 6), (1 << 15, 12, 12)])
+                                     (1 << 16, 24, 0), (1 << 16, 9, 6), (1 << 15, 12, 12), (1 << 14, 135, 4),
+                                     (1 << 14, 3, 2), (1 << 14, 13, 14)])
 def test_vs_oracle(zk, oracle, ht, nl, ls, ch):
     leaves = oracle.field_elems(ht * 1000 + nl + ls, nl * ls)
     d, c = gpu_tree(zk, leaves, ls, ch, ht)

@@ -768,6 +768,84 @@ __device__ __forceinline__ void hash_two(const uint64_t *l, const uint64_t *r, u
     }
 }
 
+// ------------------------------------------- Poseidon on two threads
+// For trees with too few leaves to fill the GPU one thread per hash, but
+// enough that six threads per hash would be issue-bound: the permutation is
+// split over the two threads of a lane pair (lanes 2k, 2k + 1; sixteen hashes
+// per warp, no idle lanes).  Thread h owns state lanes 6h .. 6h + 5.  Each
+// round: the S-box on the owned lanes (lane 0 only, on thread 0, in partial
+// rounds); then the MDS with the 32-bit halves split between the pair (thread
+// 0 takes the low halves of all 12 lanes, thread 1 the high halves: six
+// 32-bit shuffles bring the partner's halves), the half-vector layer in FP64
+// as in the one-thread path, and six 64-bit shuffles that hand each thread
+// the other half of its own lanes' outputs.  The total work is about that
+// of one thread per hash, spread over twice the threads.
+__device__ __forceinline__ uint32_t shfl_xor32(uint32_t v) { return (uint32_t)__shfl_xor_sync(0xffffffffu, (int)v, 1); }
+__device__ __forceinline__ double shfl_xor_d(double v) { return __shfl_xor_sync(0xffffffffu, v, 1); }
+
+// s: lanes 6h .. 6h + 5 (partially reduced, in and out).  Every lane of the
+// warp must call this (shuffles over the full warp).
+__device__ __forceinline__ void poseidon_permute_duo(uint64_t s[6], uint32_t h, const PoseidonTab &tab) {
+#pragma unroll
+    for (int i = 0; i < 6; i++) s[i] = pr_add_c(s[i], tab.rc0[6 * h + i]);
+#pragma unroll 1
+    for (int rnd = 0; rnd < 30; rnd++) {
+        if (rnd < 4 || rnd >= 26) {
+#pragma unroll
+            for (int i = 0; i < 6; i++) s[i] = pr_pow7(s[i]);
+        } else if (h == 0) {
+            s[0] = pr_pow7(s[0]);
+        }
+        // Half h of all 12 lanes: own lanes directly, the partner's through a shuffle.
+        double a[12], o[12];
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            const uint32_t lo = (uint32_t)s[i], hi = (uint32_t)(s[i] >> 32);
+            const uint32_t got = shfl_xor32(h ? lo : hi);  // the partner wants the half it computes
+            const uint32_t mine = h ? hi : lo;
+            a[i] = magic_in(h ? got : mine);       // lanes 0-5: thread 0's own, thread 1's received
+            a[i + 6] = magic_in(h ? mine : got);   // lanes 6-11: thread 1's own, thread 0's received
+        }
+        poseidon_mds_half(a, o, tab.mdsk.v[rnd][h]);
+        // Thread 0 keeps the low outputs of lanes 0-5 and receives their high
+        // outputs; thread 1 keeps the high outputs of lanes 6-11 and receives
+        // their low outputs.
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+            const double got = shfl_xor_d(h ? o[i] : o[i + 6]);
+            const double lo = h ? got : o[i], hi = h ? o[i + 6] : got;
+            s[i] = pr_reduce_split_nc(magic_out(lo), magic_out(hi));
+        }
+    }
+}
+
+// Sponge of n words on a lane pair (zeknox's hash_or_noop: n <= 4 copies and
+// zero-pads); `active` pairs load and store, the others compute on zeros.
+// n must be the same for all pairs of a warp.
+__device__ __forceinline__ void poseidon_hash_one_duo(const uint64_t *in, uint32_t n, uint64_t *out, bool active,
+                                                      uint32_t h, const PoseidonTab &tab) {
+    if (n <= 4) {
+        if (active && h == 0)
+            for (uint32_t i = 0; i < 4; i++) out[i] = i < n ? in[i] : 0ull;
+        return;
+    }
+    uint64_t s[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t idx = 0; idx < n; idx += 8) {
+        const uint32_t len = n - idx < 8 ? n - idx : 8;
+        if (active) {
+#pragma unroll
+            for (uint32_t i = 0; i < 6; i++) {
+                const uint32_t lane = 6 * h + i;  // rate lanes 0..7 are overwritten
+                if (lane < len) s[i] = gl_canon(in[idx + lane]);
+            }
+        }
+        poseidon_permute_duo(s, h, tab);
+    }
+    if (active && h == 0)
+#pragma unroll
+        for (int i = 0; i < 4; i++) out[i] = gl_canon(s[i]);
+}
+
 // ------------------------------------------- Poseidon on six threads
 // For the latency-bound parts (narrow tree levels, small trees) one
 // permutation is spread over a group of six consecutive lanes of a warp

@@ -99,6 +99,24 @@ __device__ __forceinline__ void load_tab(typename TabOf<H>::type &dst) {
     __syncthreads();
 }
 
+// Poseidon on two threads per hash (a lane pair): sixteen hashes per warp.
+constexpr int kDuoThreads = 128;
+
+__global__ void __launch_bounds__(kDuoThreads) merkle_leaves_duo(const uint64_t *__restrict__ leaves,
+                                                                 uint64_t n_leaves, uint32_t leaf_size,
+                                                                 uint64_t *__restrict__ out, LeafMap map) {
+    __shared__ PoseidonTab tab;  // per-thread table indices: shared memory, not the constant bank
+    load_tab<kPoseidon>(tab);
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t first = (t >> 5) << 4;  // the warp's first hash
+    if (first >= n_leaves) return;         // whole warp
+    const uint32_t h = threadIdx.x & 1;
+    const uint64_t i = t >> 1;
+    const bool active = i < n_leaves;
+    const uint64_t ii = active ? i : 0;
+    poseidon_hash_one_duo(leaves + ii * leaf_size, leaf_size, out + 4 * map.slot(ii), active, h, tab);
+}
+
 // Poseidon on six threads per hash (HexGroup): five hashes per warp.  For the
 // latency-bound cases: few leaves, narrow levels, the top of the tree.
 constexpr int kHexThreads = 128;  // 4 warps = 20 hashes per block
@@ -199,10 +217,15 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
         // bound: six threads do twice the instructions of one); 4096 nodes
         // 20 us vs 40 us.  Whole trees of 135-word leaves, six-threaded vs
         // one-threaded leaves: 8192 leaves 0.48 vs 0.65 ms, 16384 leaves 0.80
-        // vs 0.68 ms, 32768 leaves 1.43 vs 0.87 ms.
-        constexpr uint64_t kHexLeaves = 1 << 13, kHexNodes = 1 << 14;
+        // vs 0.68 ms, 32768 leaves 1.43 vs 0.87 ms.  Two threads per hash
+        // win between the two: 16384 leaves 0.59 ms (4096: 0.47, 8192: 0.49,
+        // 32768: 0.97, 65536: 1.54 vs 1.46 one-threaded).
+        constexpr uint64_t kHexLeaves = 1 << 13, kHexNodes = 1 << 14, kDuoLeaves = 1 << 14;
         if (j.n_leaves <= kHexLeaves)
             merkle_leaves_hex<<<hex_blocks(j.n_leaves), kHexThreads, 0, st>>>(j.leaves, j.n_leaves, w, j.digests, map);
+        else if (j.n_leaves <= kDuoLeaves)
+            merkle_leaves_duo<<<blocks_for(2 * j.n_leaves, kDuoThreads), kDuoThreads, 0, st>>>(j.leaves, j.n_leaves, w,
+                                                                                                j.digests, map);
         else
             merkle_leaves<H><<<blocks_for(j.n_leaves, kLeafThreads), kLeafThreads, 0, st>>>(j.leaves, j.n_leaves, w,
                                                                                              j.digests, map);
