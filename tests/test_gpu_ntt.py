@@ -70,19 +70,36 @@ def test_lde_device_buffers_and_directions(zk, oracle, lg_n, rate, batches, inve
     assert np.array_equal(_host(d_in), x)  # input untouched
 
 
-@pytest.mark.parametrize("in_dev,out_dev,batches", [(False, False, 19), (False, True, 33), (True, False, 16),
-                                                     (False, False, 135)])
-def test_lde_grouped_host_copies(zk, oracle, in_dev, out_dev, batches):
+@pytest.mark.parametrize("in_dev,out_dev,batches,pinned", [(False, False, 19, False), (False, True, 33, False),
+                                                            (True, False, 16, False), (False, False, 135, False),
+                                                            (False, True, 64, True), (False, False, 45, True)])
+def test_lde_grouped_host_copies(zk, oracle, in_dev, out_dev, batches, pinned):
     """Host buffers with >= 16 polynomials go through the grouped copy/compute
-    pipeline (uneven last group included); the result is the same LDE."""
+    pipeline (4 groups, or 8 from 32 polynomials, alternating between two
+    compute streams; uneven last group included; pageable or pinned host
+    memory); the result is the same LDE."""
+    import torch
+
     lg_n, rate = 9, 2
     x = oracle.field_elems(4000 + batches, batches << lg_n)
     exp = oracle.batch_lde(x, lg_n, rate, batches)
-    src = _dev(x) if in_dev else x
-    out = _dev(np.zeros(batches << (lg_n + rate), dtype=np.uint64)) if out_dev else np.zeros_like(exp)
-    zk.lde_batch(0, out.data_ptr() if out_dev else out.ctypes.data, src.data_ptr() if in_dev else src.ctypes.data,
-                 lg_n, _cfg(zk, batches, rate, in_dev, out_dev, True))
-    assert np.array_equal(_host(out) if out_dev else out, exp)
+    if in_dev:
+        src = _dev(x)
+    elif pinned:
+        src = torch.from_numpy(x).pin_memory()
+    else:
+        src = x
+    src_ptr = src.data_ptr() if (in_dev or pinned) else src.ctypes.data
+    if out_dev:
+        out = _dev(np.zeros(batches << (lg_n + rate), dtype=np.uint64))
+    elif pinned:
+        out = torch.zeros(batches << (lg_n + rate), dtype=torch.uint64).pin_memory()
+    else:
+        out = np.zeros_like(exp)
+    out_ptr = out.data_ptr() if (out_dev or pinned) else out.ctypes.data
+    zk.lde_batch(0, out_ptr, src_ptr, lg_n, _cfg(zk, batches, rate, in_dev, out_dev, True))
+    got = _host(out) if out_dev else (out.numpy() if pinned else out)
+    assert np.array_equal(got, exp)
 
 
 def test_lde_mixed_host_device(zk, oracle):

@@ -266,9 +266,14 @@ extern "C" RustError compute_batched_lde(size_t device_id, void *output, void *i
         require(!(cfg.are_inputs_on_device && cfg.are_outputs_on_device && (const void *)d_in == (void *)d_out),
                 "input and output must not alias");
         // Host buffers: polynomials go in groups, so that the copy of one group
-        // overlaps the transform of another (copies on the context's copy stream).
+        // overlaps the transform of another (copies on the context's copy
+        // stream).  The groups' transforms alternate between two streams, so
+        // that one group's tail overlaps the next group's start (four
+        // separate 34-polynomial transforms cost 15 % more than one of 135).
+        // Measured on 135 x 2^15 -> 2^18 from pinned memory: one stream and 4
+        // groups 1.10 ms, two streams and 4 groups 0.98 ms, 8 groups 0.91 ms.
         const uint64_t B = cfg.batches;
-        const uint64_t groups = (cfg.are_inputs_on_device && cfg.are_outputs_on_device) || B < 16 ? 1 : 4;
+        const uint64_t groups = (cfg.are_inputs_on_device && cfg.are_outputs_on_device) || B < 16 ? 1 : (B < 32 ? 4 : 8);
         const uint64_t gsz = (B + groups - 1) / std::max<uint64_t>(groups, 1);
         std::vector<cudaEvent_t> ev;
         auto event = [&](cudaStream_t st) {
@@ -280,7 +285,10 @@ extern "C" RustError compute_batched_lde(size_t device_id, void *output, void *i
         };
         try {
             cudaStream_t cs = ctx.copy_stream;
-            ZK_CUDA(cudaStreamWaitEvent(cs, event(s), 0));  // after the allocations above
+            const cudaEvent_t allocated = event(s);
+            ZK_CUDA(cudaStreamWaitEvent(cs, allocated, 0));  // after the allocations above
+            const cudaStream_t lanes[2] = {s, groups > 1 ? ctx.lane_stream : s};
+            if (groups > 1) ZK_CUDA(cudaStreamWaitEvent(lanes[1], allocated, 0));
             std::vector<cudaEvent_t> in_ready;
             for (uint64_t b0 = 0; b0 < B; b0 += gsz) {
                 const uint64_t nb = std::min(gsz, B - b0);
@@ -291,14 +299,16 @@ extern "C" RustError compute_batched_lde(size_t device_id, void *output, void *i
             size_t gi = 0;
             for (uint64_t b0 = 0; b0 < B; b0 += gsz, gi++) {
                 const uint64_t nb = std::min(gsz, B - b0);
-                ZK_CUDA(cudaStreamWaitEvent(s, in_ready[gi], 0));
+                const cudaStream_t ls = lanes[gi & 1];
+                ZK_CUDA(cudaStreamWaitEvent(ls, in_ready[gi], 0));
                 lde_device(ctx, d_out + b0 * N, d_in + b0 * n, lg_n, rb, nb, ntt_direction == inverse, cfg.with_coset,
-                           s);
+                           ls);
                 if (!cfg.are_outputs_on_device) {
-                    ZK_CUDA(cudaStreamWaitEvent(cs, event(s), 0));
+                    ZK_CUDA(cudaStreamWaitEvent(cs, event(ls), 0));
                     d2h((uint64_t *)output + b0 * N, d_out + b0 * N, nb * N * sizeof(uint64_t), cs);
                 }
             }
+            if (lanes[1] != s) ZK_CUDA(cudaStreamWaitEvent(s, event(lanes[1]), 0));  // join the second lane
             if (cfg.salt_size) {
                 salt_run(d_out + B * N, (uint64_t)cfg.salt_size * N, seed_now(), s);
                 if (!cfg.are_outputs_on_device) {
@@ -310,6 +320,7 @@ extern "C" RustError compute_batched_lde(size_t device_id, void *output, void *i
             ZK_CUDA(cudaStreamSynchronize(s));
         } catch (...) {
             cudaStreamSynchronize(ctx.copy_stream);
+            cudaStreamSynchronize(ctx.lane_stream);
             cudaStreamSynchronize(s);
             for (cudaEvent_t e : ev) cudaEventDestroy(e);
             throw;

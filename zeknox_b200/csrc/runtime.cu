@@ -92,6 +92,7 @@ DeviceCtx &device_ctx(int dev) {
         // like zeknox's per-GPU "zero" stream (native/utils/gpu_t.cuh:246-252).
         ZK_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault));
         ZK_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        ZK_CUDA(cudaStreamCreateWithFlags(&c->lane_stream, cudaStreamNonBlocking));
         // Keep freed pool memory cached between calls.
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {

@@ -83,6 +83,7 @@ struct DeviceCtx {
     int dev = -1;
     cudaStream_t stream = nullptr;       // blocking stream (orders after the legacy stream)
     cudaStream_t copy_stream = nullptr;  // host<->device copies overlapped with `stream`
+    cudaStream_t lane_stream = nullptr;  // second compute lane of the host-buffer LDE
     uint64_t *line_roots[2] = {nullptr, nullptr};  // [dir] omega_4096^j, j < 4096
     PowTable roots[2][kMaxLg + 1];       // [dir][lg]: omega_{2^lg} powers
     PowTable coset;                      // coset_gen powers
