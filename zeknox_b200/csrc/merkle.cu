@@ -3,11 +3,14 @@
 //
 // One launch hashes every leaf (one thread per leaf, sponge state in
 // registers), then one launch per tree level hashes that level's nodes across
-// all subtrees, and a last one the cap: the structure of zeknox's kernels
-// (merkle.cu:215-243).  Fusing the lower levels into the leaf kernel (a block
-// folding its tile of leaves through shared memory) measured slower on B200:
-// a block then holds its registers through the serial, mostly idle fold
-// levels, which costs more than re-reading the children from L2.
+// all subtrees, and a last one the narrow top and the cap: the structure of
+// zeknox's kernels (merkle.cu:215-243).  For Poseidon, the latency-bound
+// parts (small trees, narrow levels, the top) spread each permutation over
+// six or two threads instead (hash.cuh), with thresholds set by measurement.
+// Fusing the lower levels into the leaf kernel (a block folding its tile of
+// leaves through shared memory) measured slower on B200: a block then holds
+// its registers through the serial, mostly idle fold levels, which costs more
+// than re-reading the children from L2.
 #include <stdint.h>
 
 #include <algorithm>
