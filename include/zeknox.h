@@ -216,14 +216,15 @@ typedef struct {
  * job's outputs equal zk_commit_async's. */
 ZK_EXTERN RustError zk_commit_batch(const ZkCommitJob *jobs, uint32_t n_jobs, uint32_t n_streams, void *stream);
 
-/* Autotuner of the LDE -> leaves stage (commits, batches, the server): for
- * one shape (2^lg_n coefficients, rate_bits, batches polynomials) it times
- * every legal pass count (2 or 3) and polynomials-per-block of the leaves pass
- * on scratch data and keeps the fastest for that size and batch-size class;
- * later transforms of that class use it.  Outputs do not depend on the
- * choice.  Synchronous: call outside stream capture.  *timed receives the
- * number of candidates timed (0: already tuned, or a one-pass size).
- * zk_autotune_reset forgets every choice. */
+/* Autotuner of a commit shape (commits, batches, the server): for one shape
+ * (2^lg_n coefficients, rate_bits, batches polynomials) it times, on scratch
+ * data, every legal pass count (2 or 3) and polynomials-per-block of the
+ * LDE -> leaves pass, and for Poseidon trees of up to 2^16 leaves the six-,
+ * two- and one-thread-per-hash leaf kernels; it keeps the fastest of each for
+ * that shape class, and later commits of the class use them.  Outputs do not
+ * depend on the choices.  Synchronous: call outside stream capture.  *timed
+ * receives the number of candidates timed (0: already tuned, or nothing to
+ * tune).  zk_autotune_reset forgets every choice. */
 ZK_EXTERN RustError zk_autotune_commit(uint32_t lg_n, uint32_t rate_bits, uint32_t batches, int32_t *timed);
 ZK_EXTERN RustError zk_autotune_reset(void);
 

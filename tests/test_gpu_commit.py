@@ -203,3 +203,23 @@ def test_autotuner_choices_keep_outputs_bit_exact(zk, oracle):
         assert torch.equal(before.leaves.view(torch.int64), after.leaves.view(torch.int64))
         assert torch.equal(before.cap.view(torch.int64), after.cap.view(torch.int64))
     zk.autotune_reset()
+
+
+@pytest.mark.parametrize("lg_n,rate,b", [(10, 3, 135), (11, 3, 135), (12, 2, 9), (13, 3, 40), (12, 1, 200)])
+def test_threads_per_hash_tuning_keeps_trees_bit_exact(zk, oracle, lg_n, rate, b):
+    """Trees of up to 2^16 leaves also get their Poseidon leaf kernel (six, two
+    or one thread per hash) by measurement; whichever wins, the forest equals
+    the oracle's."""
+    import torch
+
+    zk.autotune_reset()
+    x = oracle.field_elems(4500 + lg_n + b, b << lg_n)
+    assert zk.autotune(lg_n, rate, b) >= 3  # at least the three leaf layouts
+    out = zk.commit(_dev(x).view(b, 1 << lg_n), rate, 4, 0)
+    torch.cuda.synchronize()
+    lde = oracle.batch_lde(x, lg_n, rate, b)
+    leaves = oracle.transpose_rev(lde, lg_n + rate, b)
+    dig, cap = oracle.merkle_fill(leaves, b, 4, oracle.HASH_POSEIDON)
+    assert np.array_equal(out.cap.cpu().numpy().reshape(-1), cap)
+    assert np.array_equal(out.digests.cpu().numpy().reshape(-1)[:dig.size], dig)
+    zk.autotune_reset()

@@ -14,6 +14,8 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "hash.cuh"
 #include "merkle.cuh"
@@ -188,6 +190,42 @@ inline unsigned blocks_for(uint64_t n, unsigned tpb) {
     return (unsigned)(b ? b : 1);
 }
 
+// Threads per Poseidon hash for a tree's leaves: 6 (HexGroup), 2 (lane
+// pairs) or 1.  Static thresholds, measured on trees of 135-word leaves:
+// whole trees, six- vs one-threaded leaves, 8192 leaves 0.48 vs 0.65 ms,
+// 16384 leaves 0.80 vs 0.68 ms, 32768 leaves 1.43 vs 0.87 ms; two threads per
+// hash win between the two, 16384 leaves 0.59 ms (4096: 0.47, 8192: 0.49,
+// 32768: 0.97, 65536: 1.54 vs 1.46 one-threaded).  merkle_autotune_leaves
+// replaces them by measurement per (tree size, permutations per leaf).
+constexpr uint64_t kHexLeaves = 1 << 13, kDuoLeaves = 1 << 14;
+constexpr uint64_t kLayoutTuneMax = 1 << 16;  // larger trees: one thread per hash, by a wide margin
+std::mutex g_layout_mu;
+std::map<uint64_t, uint8_t> g_layout;  // layout_key -> threads per hash
+
+uint64_t layout_key(uint64_t n_leaves, uint64_t leaf_size) {
+    const uint64_t lg = 63 - __builtin_clzll(n_leaves);
+    return (lg << 32) | ((leaf_size + 7) / 8);  // permutations per leaf
+}
+uint8_t leaf_layout(uint64_t n_leaves, uint64_t leaf_size) {
+    if (n_leaves <= kLayoutTuneMax && leaf_size > 4) {
+        std::lock_guard<std::mutex> g(g_layout_mu);
+        auto it = g_layout.find(layout_key(n_leaves, leaf_size));
+        if (it != g_layout.end()) return it->second;
+    }
+    return n_leaves <= kHexLeaves ? 6 : n_leaves <= kDuoLeaves ? 2 : 1;
+}
+void launch_poseidon_leaves(const uint64_t *leaves, uint64_t n_leaves, uint32_t w, uint64_t *out, LeafMap map,
+                            uint8_t layout, cudaStream_t st) {
+    if (layout == 6)
+        merkle_leaves_hex<<<hex_blocks(n_leaves), kHexThreads, 0, st>>>(leaves, n_leaves, w, out, map);
+    else if (layout == 2)
+        merkle_leaves_duo<<<blocks_for(2 * n_leaves, kDuoThreads), kDuoThreads, 0, st>>>(leaves, n_leaves, w, out, map);
+    else
+        merkle_leaves<kPoseidon><<<blocks_for(n_leaves, kLeafThreads), kLeafThreads, 0, st>>>(leaves, n_leaves, w, out,
+                                                                                              map);
+    ZK_CHECK_LAUNCH();
+}
+
 template <int H>
 void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
     const uint32_t w = (uint32_t)j.leaf_size;
@@ -212,27 +250,15 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
     map.lg_ls = (uint32_t)__builtin_ctzll(ls);
     map.ds = ds;
     if constexpr (H == kPoseidon) {
-        // Latency-bound parts on six threads per hash: trees of at most
-        // kHexLeaves leaves, levels of fewer than kHexNodes nodes, and the
-        // top (<= 32 nodes per subtree, so that one SM per subtree stays
-        // latency- rather than issue-bound) in one launch.  Measured per
-        // level: 16384 nodes 46 us six-threaded vs 40 us one-threaded (issue
-        // bound: six threads do twice the instructions of one); 4096 nodes
-        // 20 us vs 40 us.  Whole trees of 135-word leaves, six-threaded vs
-        // one-threaded leaves: 8192 leaves 0.48 vs 0.65 ms, 16384 leaves 0.80
-        // vs 0.68 ms, 32768 leaves 1.43 vs 0.87 ms.  Two threads per hash
-        // win between the two: 16384 leaves 0.59 ms (4096: 0.47, 8192: 0.49,
-        // 32768: 0.97, 65536: 1.54 vs 1.46 one-threaded).
-        constexpr uint64_t kHexLeaves = 1 << 13, kHexNodes = 1 << 14, kDuoLeaves = 1 << 14;
-        if (j.n_leaves <= kHexLeaves)
-            merkle_leaves_hex<<<hex_blocks(j.n_leaves), kHexThreads, 0, st>>>(j.leaves, j.n_leaves, w, j.digests, map);
-        else if (j.n_leaves <= kDuoLeaves)
-            merkle_leaves_duo<<<blocks_for(2 * j.n_leaves, kDuoThreads), kDuoThreads, 0, st>>>(j.leaves, j.n_leaves, w,
-                                                                                                j.digests, map);
-        else
-            merkle_leaves<H><<<blocks_for(j.n_leaves, kLeafThreads), kLeafThreads, 0, st>>>(j.leaves, j.n_leaves, w,
-                                                                                             j.digests, map);
-        ZK_CHECK_LAUNCH();
+        // Latency-bound parts on several threads per hash: the leaves of
+        // small trees (leaf_layout), levels of fewer than kHexNodes nodes,
+        // and the top (<= 32 nodes per subtree, so that one SM per subtree
+        // stays latency- rather than issue-bound) in one launch.  Measured
+        // per level: 16384 nodes 46 us six-threaded vs 40 us one-threaded
+        // (issue bound: six threads do twice the instructions of one); 4096
+        // nodes 20 us vs 40 us.
+        constexpr uint64_t kHexNodes = 1 << 14;
+        launch_poseidon_leaves(j.leaves, j.n_leaves, w, j.digests, map, leaf_layout(j.n_leaves, w), st);
         uint32_t lg_top = 0;
         while (lg_top + 1 < map.lg_ls && lg_top < 5 && (j.n_caps << (lg_top + 1)) < kHexNodes) lg_top++;
         for (uint32_t lg_w = map.lg_ls - 1; lg_w > lg_top; lg_w--) {
@@ -332,6 +358,61 @@ void merkle_open(const uint64_t *leaves, const uint64_t *digests, uint64_t n_lea
     merkle_open_paths<<<grid_for(n_queries * lg_ls), 256, 0, st>>>(digests, n_leaves, lg_ls, 2 * ls - 2, idx, n_queries,
                                                                    out_siblings);
     ZK_CHECK_LAUNCH();
+}
+
+int merkle_autotune_leaves(uint64_t n_leaves, uint64_t leaf_size, uint64_t hash_type, cudaStream_t s) {
+    if (hash_type != kPoseidon || leaf_size <= 4 || n_leaves < 2 || n_leaves > kLayoutTuneMax) return 0;
+    require(leaf_size < (1ull << 31), "invalid leaf size");
+    const uint64_t key = layout_key(n_leaves, leaf_size);
+    {
+        std::lock_guard<std::mutex> g(g_layout_mu);
+        if (g_layout.count(key)) return 0;
+    }
+    // Zero leaves (canonical) of the class's own shape; digests in direct order.
+    uint64_t *leaves = nullptr, *out = nullptr;
+    ZK_CUDA(cudaMallocAsync((void **)&leaves, n_leaves * leaf_size * sizeof(uint64_t), s));
+    ZK_CUDA(cudaMallocAsync((void **)&out, n_leaves * 4 * sizeof(uint64_t), s));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    uint8_t best = 1;
+    float best_ms = 1e30f;
+    int timed = 0;
+    try {
+        ZK_CUDA(cudaMemsetAsync(leaves, 0, n_leaves * leaf_size * sizeof(uint64_t), s));
+        ZK_CUDA(cudaEventCreate(&e0));
+        ZK_CUDA(cudaEventCreate(&e1));
+        const LeafMap direct{};
+        for (uint8_t layout : {6, 2, 1}) {
+            launch_poseidon_leaves(leaves, n_leaves, (uint32_t)leaf_size, out, direct, layout, s);  // warm-up
+            ZK_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < 3; r++)
+                launch_poseidon_leaves(leaves, n_leaves, (uint32_t)leaf_size, out, direct, layout, s);
+            ZK_CUDA(cudaEventRecord(e1, s));
+            ZK_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            ZK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            timed++;
+            if (ms < best_ms) best_ms = ms, best = layout;
+        }
+    } catch (...) {
+        cudaStreamSynchronize(s);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        cudaFreeAsync(leaves, s);
+        cudaFreeAsync(out, s);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ZK_CUDA(cudaFreeAsync(leaves, s));
+    ZK_CUDA(cudaFreeAsync(out, s));
+    std::lock_guard<std::mutex> g(g_layout_mu);
+    g_layout[key] = best;
+    return timed;
+}
+
+void merkle_autotune_clear() {
+    std::lock_guard<std::mutex> g(g_layout_mu);
+    g_layout.clear();
 }
 
 bool merkle_hash_supported(uint64_t ht) {

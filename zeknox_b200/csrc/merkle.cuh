@@ -17,6 +17,14 @@ struct MerkleJob {
 bool merkle_hash_supported(uint64_t hash_type);
 void merkle_validate(const MerkleJob &job);  // throws zk::Error
 void merkle_run(const MerkleJob &job, cudaStream_t s);
+// Threads-per-hash autotuner for Poseidon leaves: times the six-, two- and
+// one-thread leaf kernels on a zero tree of this shape (n_leaves <= 2^16,
+// leaf_size > 4; other shapes and hashers return 0) and keeps the fastest for
+// its class (log2 of the leaf count, permutations per leaf).  Returns the
+// number of candidates timed (0: already tuned or not tunable).  Outputs do
+// not depend on the choice.
+int merkle_autotune_leaves(uint64_t n_leaves, uint64_t leaf_size, uint64_t hash_type, cudaStream_t s);
+void merkle_autotune_clear();
 // Leaf rows and sibling paths of n_queries leaves (all pointers on the device).
 void merkle_open(const uint64_t *leaves, const uint64_t *digests, uint64_t n_leaves, uint64_t leaf_size,
                  uint64_t cap_height, const uint64_t *idx, uint64_t n_queries, uint64_t *out_leaves,

@@ -210,13 +210,17 @@ extern "C" RustError zk_autotune_commit(uint32_t lg_n, uint32_t rate_bits, uint3
         DeviceCtx &ctx = device_ctx(dev);
         root_table(ctx, lg_n + rate_bits, false);
         line_roots(ctx, false);
-        const int n = ntt_autotune_leaves(lg_n, rate_bits, batches, ctx.stream);
+        int n = ntt_autotune_leaves(lg_n, rate_bits, batches, ctx.stream);
+        n += merkle_autotune_leaves(1ull << (lg_n + rate_bits), batches, 0, ctx.stream);  // Poseidon leaves
         if (timed) *timed = n;
     });
 }
 
 extern "C" RustError zk_autotune_reset(void) {
-    return guard([&] { ntt_autotune_clear(); });
+    return guard([&] {
+        ntt_autotune_clear();
+        merkle_autotune_clear();
+    });
 }
 
 // ------------------------------------------------------------------ server
