@@ -27,6 +27,17 @@ namespace {
 
 constexpr int kLeafThreads = 128;
 
+// Programmatic dependent launch: the level and top kernels are launched with
+// the programmatic-serialization attribute (launch_after below), so each may
+// start while the kernel before it on the stream drains.  A kernel first does
+// what does not depend on that kernel (its round tables into shared memory),
+// then waits with griddepcontrol.wait until the previous grid has completed
+// and its writes are visible; every kernel of the chain signals
+// launch_dependents once its block has stored its outputs.  Both
+// instructions are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Digest slot of leaf i: subtree s = i / Ls owns [s*Ds, (s+1)*Ds); its leaves
 // sit at the tail, Ds - Ls + j.  In direct mode digest i goes to slot i.
 struct LeafMap {
@@ -49,6 +60,7 @@ __global__ void __launch_bounds__(kLeafThreads) merkle_leaves(const uint64_t *__
     // S-box width: all 12 lanes at once measured faster for Poseidon; for
     // Poseidon2 the larger loop body costs more in instruction fetch.
     hash_one<H, H == kPoseidon ? 12 : 4>(leaves + i * leaf_size, leaf_size, out + 4 * map.slot(i));
+    pdl_release();
 }
 
 // One level of width w = 2^lg_w nodes per subtree (at offsets w - 2 .. 2w - 3
@@ -61,7 +73,9 @@ __global__ void __launch_bounds__(kLeafThreads) merkle_level(uint64_t *__restric
     if (tid >= (n_caps << lg_w)) return;
     const uint64_t s = tid >> lg_w, i = (w - 2) + (tid & (w - 1));
     uint64_t *base = digests + 4 * s * ds;
+    pdl_wait();
     hash_two<H, W>(base + 4 * (2 * i + 2), base + 4 * (2 * i + 3), base + 4 * i);
+    pdl_release();
 }
 
 // One block per subtree: the levels of width w_top, w_top/2, ..., 1 (the cap),
@@ -83,6 +97,7 @@ __global__ void __launch_bounds__(256) merkle_top(uint64_t *__restrict__ digests
     __syncthreads();
     const uint64_t sub = blockIdx.x;
     uint64_t *base = digests + 4 * sub * ds;
+    pdl_wait();
     for (uint32_t w = w_top; w >= 1; w >>= 1) {
         const uint32_t i = threadIdx.x;
         if (i < w) {
@@ -120,6 +135,7 @@ __global__ void __launch_bounds__(kDuoThreads) merkle_leaves_duo(const uint64_t 
     const bool active = i < n_leaves;
     const uint64_t ii = active ? i : 0;
     poseidon_hash_one_duo(leaves + ii * leaf_size, leaf_size, out + 4 * map.slot(ii), active, h, tab);
+    pdl_release();
 }
 
 // Poseidon on six threads per hash (HexGroup): five hashes per warp.  For the
@@ -139,6 +155,7 @@ __global__ void __launch_bounds__(kHexThreads) merkle_leaves_hex(const uint64_t 
     const bool active = g.real() && i < n_leaves;
     const uint64_t ii = active ? i : 0;
     poseidon_hash_one_hex(leaves + ii * leaf_size, leaf_size, out + 4 * map.slot(ii), active, g, tab);
+    pdl_release();
 }
 
 __global__ void __launch_bounds__(kHexThreads) merkle_level_hex(uint64_t *__restrict__ digests, uint32_t lg_w,
@@ -154,7 +171,9 @@ __global__ void __launch_bounds__(kHexThreads) merkle_level_hex(uint64_t *__rest
     const uint64_t tt = active ? tid : 0;
     const uint64_t sub = tt >> lg_w, i = (w - 2) + (tt & (w - 1));
     uint64_t *base = digests + 4 * sub * ds;
+    pdl_wait();
     poseidon_hash_two_hex(base + 4 * (2 * i + 2), base + 4 * (2 * i + 3), base + 4 * i, active, g, tab);
+    pdl_release();
 }
 
 // One block per subtree: levels of width w_top (<= 32) .. 1, then the cap.
@@ -166,6 +185,7 @@ __global__ void __launch_bounds__(224) merkle_top_hex(uint64_t *__restrict__ dig
     const uint64_t sub = blockIdx.x;
     uint64_t *base = digests + 4 * sub * ds;
     const uint32_t node = (threadIdx.x >> 5) * 5 + g.group_in_warp();
+    pdl_wait();
     for (uint32_t w = w_top; w >= 1; w >>= 1) {
         if ((threadIdx.x >> 5) * 5 < w) {  // warps with at least one node of this level
             const bool active = g.real() && node < w;
@@ -188,6 +208,24 @@ inline unsigned blocks_for(uint64_t n, unsigned tpb) {
     const uint64_t b = (n + tpb - 1) / tpb;
     require(b < (1ull << 31), "Merkle launch too large");
     return (unsigned)(b ? b : 1);
+}
+
+// Launch a level or top kernel so that it may start while the previous
+// kernel on `st` drains (it calls pdl_wait before reading that kernel's output).
+template <typename... P, typename... A>
+void launch_after(void (*kern)(P...), unsigned grid, unsigned block, cudaStream_t st, A... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    ZK_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+    ZK_CHECK_LAUNCH();
 }
 
 // Threads per Poseidon hash for a tree's leaves: 6 (HexGroup), 2 (lane
@@ -264,16 +302,14 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
         for (uint32_t lg_w = map.lg_ls - 1; lg_w > lg_top; lg_w--) {
             const uint64_t nodes = j.n_caps << lg_w;
             if (nodes >= kHexNodes)  // 12-lane S-box, as in the leaves (measured 15 us faster per tree of 2^18)
-                merkle_level<H, 12><<<blocks_for(nodes, kLeafThreads), kLeafThreads, 0, st>>>(j.digests, lg_w,
-                                                                                              j.n_caps, ds);
+                launch_after(merkle_level<H, 12>, blocks_for(nodes, kLeafThreads), kLeafThreads, st, j.digests, lg_w,
+                             j.n_caps, ds);
             else
-                merkle_level_hex<<<hex_blocks(nodes), kHexThreads, 0, st>>>(j.digests, lg_w, j.n_caps, ds);
-            ZK_CHECK_LAUNCH();
+                launch_after(merkle_level_hex, hex_blocks(nodes), kHexThreads, st, j.digests, lg_w, j.n_caps, ds);
         }
         require(j.n_caps < (1ull << 31), "too many subtrees");
         const uint32_t w_top = 1u << lg_top;
-        merkle_top_hex<<<(unsigned)j.n_caps, 32 * ((w_top + 4) / 5), 0, st>>>(j.digests, j.cap, ds, w_top);
-        ZK_CHECK_LAUNCH();
+        launch_after(merkle_top_hex, (unsigned)j.n_caps, 32 * ((w_top + 4) / 5), st, j.digests, j.cap, ds, w_top);
         return;
     }
     merkle_leaves<H><<<blocks_for(j.n_leaves, kLeafThreads), kLeafThreads, 0, st>>>(j.leaves, j.n_leaves, w, j.digests,
@@ -285,15 +321,12 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
     constexpr uint64_t kNarrow = 1 << 14;
     uint32_t lg_top = 0;
     while (lg_top + 1 < map.lg_ls && lg_top < 8 && (j.n_caps << (lg_top + 1)) < kNarrow) lg_top++;
-    for (uint32_t lg_w = map.lg_ls - 1; lg_w > lg_top; lg_w--) {
-        merkle_level<H, 4><<<blocks_for(j.n_caps << lg_w, kLeafThreads), kLeafThreads, 0, st>>>(j.digests, lg_w,
-                                                                                                 j.n_caps, ds);
-        ZK_CHECK_LAUNCH();
-    }
+    for (uint32_t lg_w = map.lg_ls - 1; lg_w > lg_top; lg_w--)
+        launch_after(merkle_level<H, 4>, blocks_for(j.n_caps << lg_w, kLeafThreads), kLeafThreads, st, j.digests, lg_w,
+                     j.n_caps, ds);
     require(j.n_caps < (1ull << 31), "too many subtrees");
     const uint32_t w_top = 1u << lg_top;
-    merkle_top<H><<<(unsigned)j.n_caps, std::max<uint32_t>(32, w_top), 0, st>>>(j.digests, j.cap, ds, w_top);
-    ZK_CHECK_LAUNCH();
+    launch_after(merkle_top<H>, (unsigned)j.n_caps, std::max<uint32_t>(32, w_top), st, j.digests, j.cap, ds, w_top);
 }
 
 }  // namespace
