@@ -19,6 +19,7 @@
 
 #include "hash.cuh"
 #include "merkle.cuh"
+#include "pdl.cuh"
 #include "runtime.cuh"
 
 namespace zk {
@@ -27,16 +28,9 @@ namespace {
 
 constexpr int kLeafThreads = 128;
 
-// Programmatic dependent launch: the level and top kernels are launched with
-// the programmatic-serialization attribute (launch_after below), so each may
-// start while the kernel before it on the stream drains.  A kernel first does
-// what does not depend on that kernel (its round tables into shared memory),
-// then waits with griddepcontrol.wait until the previous grid has completed
-// and its writes are visible; every kernel of the chain signals
-// launch_dependents once its block has stored its outputs.  Both
-// instructions are no-ops for a kernel launched without the attribute.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+// The level and top kernels are launched with launch_after (pdl.cuh): each
+// loads its round tables, waits for the previous level, and releases its
+// dependents once its block has stored its nodes.
 
 // Digest slot of leaf i: subtree s = i / Ls owns [s*Ds, (s+1)*Ds); its leaves
 // sit at the tail, Ds - Ls + j.  In direct mode digest i goes to slot i.
@@ -210,23 +204,6 @@ inline unsigned blocks_for(uint64_t n, unsigned tpb) {
     return (unsigned)(b ? b : 1);
 }
 
-// Launch a level or top kernel so that it may start while the previous
-// kernel on `st` drains (it calls pdl_wait before reading that kernel's output).
-template <typename... P, typename... A>
-void launch_after(void (*kern)(P...), unsigned grid, unsigned block, cudaStream_t st, A... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    ZK_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
-    ZK_CHECK_LAUNCH();
-}
 
 // Threads per Poseidon hash for a tree's leaves: 6 (HexGroup), 2 (lane
 // pairs) or 1.  Static thresholds, measured on trees of 135-word leaves:
@@ -302,14 +279,15 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
         for (uint32_t lg_w = map.lg_ls - 1; lg_w > lg_top; lg_w--) {
             const uint64_t nodes = j.n_caps << lg_w;
             if (nodes >= kHexNodes)  // 12-lane S-box, as in the leaves (measured 15 us faster per tree of 2^18)
-                launch_after(merkle_level<H, 12>, blocks_for(nodes, kLeafThreads), kLeafThreads, st, j.digests, lg_w,
-                             j.n_caps, ds);
+                launch_after(merkle_level<H, 12>, blocks_for(nodes, kLeafThreads), kLeafThreads, 0, st, j.digests,
+                             lg_w, j.n_caps, ds);
             else
-                launch_after(merkle_level_hex, hex_blocks(nodes), kHexThreads, st, j.digests, lg_w, j.n_caps, ds);
+                launch_after(merkle_level_hex, hex_blocks(nodes), kHexThreads, 0, st, j.digests, lg_w, j.n_caps, ds);
         }
         require(j.n_caps < (1ull << 31), "too many subtrees");
         const uint32_t w_top = 1u << lg_top;
-        launch_after(merkle_top_hex, (unsigned)j.n_caps, 32 * ((w_top + 4) / 5), st, j.digests, j.cap, ds, w_top);
+        launch_after(merkle_top_hex, (unsigned)j.n_caps, 32 * ((w_top + 4) / 5), 0, st, j.digests, j.cap, ds,
+                     w_top);
         return;
     }
     merkle_leaves<H><<<blocks_for(j.n_leaves, kLeafThreads), kLeafThreads, 0, st>>>(j.leaves, j.n_leaves, w, j.digests,
@@ -322,11 +300,12 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
     uint32_t lg_top = 0;
     while (lg_top + 1 < map.lg_ls && lg_top < 8 && (j.n_caps << (lg_top + 1)) < kNarrow) lg_top++;
     for (uint32_t lg_w = map.lg_ls - 1; lg_w > lg_top; lg_w--)
-        launch_after(merkle_level<H, 4>, blocks_for(j.n_caps << lg_w, kLeafThreads), kLeafThreads, st, j.digests, lg_w,
-                     j.n_caps, ds);
+        launch_after(merkle_level<H, 4>, blocks_for(j.n_caps << lg_w, kLeafThreads), kLeafThreads, 0, st, j.digests,
+                     lg_w, j.n_caps, ds);
     require(j.n_caps < (1ull << 31), "too many subtrees");
     const uint32_t w_top = 1u << lg_top;
-    launch_after(merkle_top<H>, (unsigned)j.n_caps, std::max<uint32_t>(32, w_top), st, j.digests, j.cap, ds, w_top);
+    launch_after(merkle_top<H>, (unsigned)j.n_caps, std::max<uint32_t>(32, w_top), 0, st, j.digests, j.cap, ds,
+                 w_top);
 }
 
 }  // namespace

@@ -25,6 +25,7 @@
 
 #include "gl64.cuh"
 #include "ntt.cuh"
+#include "pdl.cuh"
 #include "runtime.cuh"
 
 namespace zk {
@@ -217,6 +218,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
     uint64_t *tw = smem;  // omega_L^e, e < L
     uint64_t *sm = smem + L;
     for (uint32_t j = threadIdx.x; j < L; j += blockDim.x) tw[j] = __ldg(a.line_roots + (j << (kLineLgMax - l)));
+    pdl_wait();  // the previous pass's output (launch_after) is read and overwritten only from here on
     const uint64_t g = blockIdx.x;
 
     if (a.kind == 0) {
@@ -380,6 +382,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_last_pass_leaves(PassArgs a) 
     uint64_t *tw = smem;
     uint64_t *sm = smem + L;
     for (uint32_t j = threadIdx.x; j < L; j += blockDim.x) tw[j] = __ldg(a.line_roots + (j << (kLineLgMax - l)));
+    pdl_wait();  // the previous pass's output is read only from here on
     const uint64_t Q = 1ull << a.lg_pre;
     const uint64_t krev = blockIdx.x % Q, pg = blockIdx.x / Q;
     const uint64_t p0 = pg << a.lg_t;  // first polynomial of the group (within the chunk)
@@ -505,7 +508,9 @@ size_t pass_smem(uint32_t l, uint32_t lg_t) {
     return (size_t)(L + L * tp) * sizeof(uint64_t);
 }
 
-void launch_pass(const PassArgs &a, uint64_t groups, cudaStream_t s) {
+// after_pass: the previous launch on `s` is the pass before this one of the
+// same transform, so this pass may start while it drains (pdl.cuh).
+void launch_pass(const PassArgs &a, uint64_t groups, cudaStream_t s, bool after_pass) {
     const size_t smem = pass_smem(a.l, a.lg_t);
     static std::atomic<uint64_t> attr_set{0};  // one bit per device
     const int dev = current_device();
@@ -514,6 +519,10 @@ void launch_pass(const PassArgs &a, uint64_t groups, cudaStream_t s) {
         attr_set.fetch_or(1ull << dev);
     }
     require(groups < (1ull << 31), "transform too large for one launch");
+    if (after_pass) {
+        launch_after(ntt_pass_kernel, (unsigned)groups, kNttThreads, smem, s, a);
+        return;
+    }
     ntt_pass_kernel<<<(unsigned)groups, kNttThreads, smem, s>>>(a);
     ZK_CHECK_LAUNCH();
 }
@@ -527,8 +536,7 @@ void launch_leaves_pass(const PassArgs &a, uint64_t groups, cudaStream_t s) {
         attr_set.fetch_or(1ull << dev);
     }
     require(groups < (1ull << 31), "transform too large for one launch");
-    ntt_last_pass_leaves<<<(unsigned)groups, kNttThreads, smem, s>>>(a);
-    ZK_CHECK_LAUNCH();
+    launch_after(ntt_last_pass_leaves, (unsigned)groups, kNttThreads, smem, s, a);  // always after a pass
 }
 
 }  // namespace
@@ -628,7 +636,7 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
             a.lg_t = std::min<uint32_t>(a.lg_t, 4);
         }
         const uint64_t groups = (j.batches + (1ull << a.lg_t) - 1) >> a.lg_t;
-        launch_pass(a, groups, s);
+        launch_pass(a, groups, s, false);
         return;
     }
 
@@ -666,7 +674,7 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
                 a.post_lo = nullptr;
                 a.scale = 1;
                 const uint64_t groups = nb << (lg - a.l - a.lg_t);
-                launch_pass(a, groups, s);
+                launch_pass(a, groups, s, p > 0);
             } else if (j.to_leaves) {
                 // 8 polynomials per block: 64-byte runs in every leaf row (more resident
                 // blocks hide the loads of the intermediate better than 16 did)
@@ -696,7 +704,7 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
                 a.pre_lo = nullptr;
                 a.n_valid = N;
                 const uint64_t groups = nb << (a.lg_pre - a.lg_t);
-                launch_pass(a, groups, s);
+                launch_pass(a, groups, s, true);
             }
         }
     }
@@ -783,7 +791,7 @@ void ntt_run_on_tables(const NttJob &j, const PowTable &roots, const uint64_t *l
         a.src_poly_stride = j.src_stride;
         a.dst_poly_stride = j.dst_stride;
         a.n_valid = j.n_valid;
-        launch_pass(a, (j.batches + (1ull << a.lg_t) - 1) >> a.lg_t, s);
+        launch_pass(a, (j.batches + (1ull << a.lg_t) - 1) >> a.lg_t, s, false);
         return;
     }
     const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(j.batches, j.scratch_elems / N));
@@ -809,7 +817,7 @@ void ntt_run_on_tables(const NttJob &j, const PowTable &roots, const uint64_t *l
                 a.dst_poly_stride = N;
                 a.post_lo = nullptr;
                 a.scale = 1;
-                launch_pass(a, nb << (lg - a.l - a.lg_t), s);
+                launch_pass(a, nb << (lg - a.l - a.lg_t), s, p > 0);
             } else {
                 a.kind = 1;
                 a.lg_s = 0;
@@ -821,7 +829,7 @@ void ntt_run_on_tables(const NttJob &j, const PowTable &roots, const uint64_t *l
                 a.dst_poly_stride = j.dst_stride;
                 a.pre_lo = nullptr;
                 a.n_valid = N;
-                launch_pass(a, nb << (a.lg_pre - a.lg_t), s);
+                launch_pass(a, nb << (a.lg_pre - a.lg_t), s, true);
             }
         }
     }
