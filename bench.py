@@ -236,6 +236,7 @@ def main() -> None:
     ap.add_argument("--workload", default="commit", choices=["commit", "merkle", "sweep", "batched", "served", "fri"],
                     help="commit (default, the bench line); the others print their own JSON summary")
     ap.add_argument("--jobs", type=int, default=0)
+    ap.add_argument("--leaves", type=int, default=8192, help="leaf count of the merkle workload (a power of two)")
     ap.add_argument("--streams", type=int, default=4)
     ap.add_argument("--budget-gb", type=int, default=120)
     ap.add_argument("--rates", type=float, nargs="*", default=[0.25, 0.5, 0.75, 1.0, 1.25])
@@ -484,12 +485,14 @@ def _ev_ms(torch, fn, reps=1):
 
 
 def run_merkle_only(args):
-    """Plain Poseidon Merkle tree, 8192 leaves x 135, cap height 4 (the reference's own CPU-runnable case)."""
+    """Plain Poseidon Merkle tree, 8192 leaves x 135, cap height 4 (the reference's own CPU-runnable case);
+    --leaves picks another power-of-two leaf count of the same width."""
     import torch
 
     import zeknox_b200 as zk
 
-    nl, w, ch = 8192, 135, 4
+    nl, w, ch = args.leaves, 135, 4
+    assert nl >= 32 and nl & (nl - 1) == 0, "--leaves must be a power of two >= 32"
     host = field_elems(0x5EED0001, nl * w)
     leaves = torch.from_numpy(host).cuda().view(nl, w)
     d, c = zk.merkle_tree(leaves, ch, 0)
@@ -497,8 +500,11 @@ def run_merkle_only(args):
         zk.merkle_tree(leaves, ch, 0, d, c)
     ms = _ev_ms(torch, lambda: zk.merkle_tree(leaves, ch, 0, d, c), args.steps)
     perms = nl * 17 + nl
-    out = {"workload": "merkle 8192x135 poseidon cap_height 4", "ms": ms, "perm_per_s": perms / (ms * 1e-3),
+    out = {"workload": f"merkle {nl}x135 poseidon cap_height 4", "ms": ms, "perm_per_s": perms / (ms * 1e-3),
            "leaf_elems_per_s": nl * w / (ms * 1e-3)}
+    if args.no_cpu_baseline:
+        print(json.dumps(out), flush=True)
+        return
     from oracle import oracle as O
 
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
