@@ -1,0 +1,146 @@
+"""GPU parity and speed against zeknox's own sm_100a build (oracle/_ref, compiled
+from zeknox's sources) at full benchmark sizes, on the same B200 and the same
+device buffers:
+
+* the default commit (135 x 2^15 coefficients, rate 3, Poseidon, cap 4)
+  through the drop-in ABI: compute_batched_lde -> compute_transpose_rev ->
+  fill_digests_buf_linear_gpu_with_gpu_ptr, every output compared word for
+  word (LDE matrix, leaves, digests, cap);
+* the hash sweep's trees (2^20 leaves x 135, cap 4) for Poseidon, Poseidon2
+  and Keccak, digests and cap compared.
+
+Each phase is timed with CUDA events (one warm-up, then the mean of a few
+runs).  With ZK_SPEED_OUT set, the timings are written there as JSON lines.
+The speed assertion only guards against regressions (this library must not be
+slower than the reference build); the numbers themselves are the record.
+"""
+
+import ctypes
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def zk():
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import zeknox_b200 as zk
+
+    return zk
+
+
+@pytest.fixture(scope="module")
+def ref():
+    from oracle.oracle import HERE
+
+    so = HERE / "_ref" / "libzkref_gpu.so"
+    if not so.exists():
+        pytest.skip("zeknox sm_100a build not present (oracle/build_ref.sh)")
+    from zeknox_b200.capi import NTTConfig, RustError, TransposeConfig
+
+    L = ctypes.CDLL(str(so))
+    vp, sz, u32, u64 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64
+    L.init_twiddle_factors.argtypes = [sz, sz]
+    L.init_twiddle_factors.restype = RustError
+    L.init_coset.argtypes = [sz, sz, u64]
+    L.init_coset.restype = RustError
+    L.compute_batched_lde.argtypes = [sz, vp, vp, u32, ctypes.c_int, NTTConfig]
+    L.compute_batched_lde.restype = RustError
+    L.compute_transpose_rev.argtypes = [sz, vp, vp, u32, TransposeConfig]
+    L.compute_transpose_rev.restype = RustError
+    L.fill_digests_buf_linear_gpu_with_gpu_ptr.argtypes = [vp, vp, vp, u64, u64, u64, u64, u64, u64, u64]
+    L.fill_digests_buf_linear_gpu_with_gpu_ptr.restype = None
+    return L
+
+
+def _timed(fn, reps=3):
+    """Mean device time (ms) of fn() over reps runs after one warm-up; fn may
+    synchronise internally (the drop-in ABI's NTT calls do)."""
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def _record(entry):
+    path = os.environ.get("ZK_SPEED_OUT")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps(entry) + "\n")
+
+
+def test_default_commit_equals_and_outruns_the_reference_build(zk, ref, oracle):
+    import torch
+
+    b, lg_n, rate, ch = 135, 15, 3, 4
+    lg = lg_n + rate
+    n, N = 1 << lg_n, 1 << lg
+    nd, nc = 2 * (N - (1 << ch)), 1 << ch
+    x = torch.from_numpy(oracle.field_elems(0x5EED0002, b * n)).cuda()
+    cfg = zk.NTTConfig.default()
+    cfg.batches, cfg.extension_rate_bits, cfg.with_coset = b, rate, True
+    cfg.are_inputs_on_device = cfg.are_outputs_on_device = True
+    tcfg = zk.TransposeConfig.default()
+    tcfg.batches, tcfg.are_inputs_on_device, tcfg.are_outputs_on_device = b, True, True
+    assert ref.init_twiddle_factors(0, lg).code == 0
+    assert ref.init_coset(0, lg, 7).code == 0
+
+    def buffers():
+        return (torch.empty(b * N, dtype=torch.uint64, device="cuda"), torch.empty(b * N, dtype=torch.uint64, device="cuda"),
+                torch.zeros(nd * 4, dtype=torch.uint64, device="cuda"), torch.zeros(nc * 4, dtype=torch.uint64, device="cuda"))
+
+    times = {}
+    outs = {}
+    for name, lib, check in (("reference", ref, lambda r: r.code == 0), ("ours", zk.capi.LIB, lambda r: r.code == 0)):
+        lde, leaves, dig, cap = buffers()
+        t_lde = _timed(lambda: check(lib.compute_batched_lde(0, lde.data_ptr(), x.data_ptr(), lg_n, 0, cfg)) or
+                       pytest.fail(f"{name} LDE failed"))
+        t_tr = _timed(lambda: check(lib.compute_transpose_rev(0, leaves.data_ptr(), lde.data_ptr(), lg, tcfg)) or
+                      pytest.fail(f"{name} transpose failed"))
+        t_mk = _timed(lambda: lib.fill_digests_buf_linear_gpu_with_gpu_ptr(dig.data_ptr(), cap.data_ptr(),
+                                                                           leaves.data_ptr(), nd, nc, N, b, ch, 0, 0))
+        torch.cuda.synchronize()
+        times[name] = {"lde_ms": t_lde, "transpose_ms": t_tr, "merkle_ms": t_mk, "total_ms": t_lde + t_tr + t_mk}
+        outs[name] = (lde, leaves, dig, cap)
+    for k, what in enumerate(("LDE matrix", "leaves", "digests", "cap")):
+        assert torch.equal(outs["ours"][k].view(torch.int64), outs["reference"][k].view(torch.int64)), what
+    entry = {"case": "commit 135 x 2^15, rate 3, poseidon, cap 4 (drop-in ABI, device buffers)", **times,
+             "speedup": {k: times["reference"][k] / times["ours"][k] for k in times["ours"]}}
+    _record(entry)
+    assert times["ours"]["total_ms"] <= times["reference"]["total_ms"], entry
+
+
+@pytest.mark.parametrize("ht", [0, 3, 1])
+def test_sweep_trees_equal_and_outrun_the_reference_build(zk, ref, ht):
+    import torch
+
+    nl, w, ch = 1 << 20, 135, 4
+    nd, nc = 2 * (nl - (1 << ch)), 1 << ch
+    g = torch.Generator(device="cuda").manual_seed(0x5EED0004)
+    leaves = torch.randint(0, 2**62, (nl * w,), generator=g, device="cuda", dtype=torch.int64).view(torch.uint64)
+    res = {}
+    for name, fill in (("reference", ref.fill_digests_buf_linear_gpu_with_gpu_ptr),
+                       ("ours", zk.capi.LIB.fill_digests_buf_linear_gpu_with_gpu_ptr)):
+        dig = torch.zeros(nd * 4, dtype=torch.uint64, device="cuda")
+        cap = torch.zeros(nc * 4, dtype=torch.uint64, device="cuda")
+        t = _timed(lambda: fill(dig.data_ptr(), cap.data_ptr(), leaves.data_ptr(), nd, nc, nl, w, ch, ht, 0), reps=2)
+        res[name] = (t, dig, cap)
+    assert torch.equal(res["ours"][2].view(torch.int64), res["reference"][2].view(torch.int64))
+    assert torch.equal(res["ours"][1].view(torch.int64), res["reference"][1].view(torch.int64))
+    entry = {"case": f"merkle 2^20 x 135, cap 4, hash type {ht}", "reference_ms": res["reference"][0],
+             "ours_ms": res["ours"][0], "speedup": res["reference"][0] / res["ours"][0]}
+    _record(entry)
+    assert res["ours"][0] <= res["reference"][0], entry
