@@ -255,3 +255,68 @@ def test_opening_out_of_range_index(zk, oracle):
     rows, sib = rows.cpu().numpy(), sib.cpu().numpy()
     assert (rows[1] == np.uint64(2**64 - 1)).all() and (sib[1] == np.uint64(2**64 - 1)).all()
     assert np.array_equal(rows[0], leaves[5 * ls:6 * ls]) and np.array_equal(rows[2], leaves[127 * ls:128 * ls])
+
+
+# ---------------------------------------- Monolith: Bars need canonical inputs
+def _monolith_mds_row():
+    import re
+    from pathlib import Path
+
+    h = (Path(__file__).resolve().parents[1] / "zeknox_b200" / "csrc" / "zk_constants.h").read_text()
+    m = re.search(r"#define ZK_MONOLITH_MDS_ROW_LIST \\\n(.*?)\nZK_CONST_TABLE", h, re.S)
+    return [int(x, 16) for x in re.findall(r"0x[0-9a-f]+", m.group(1))]
+
+
+def _leaves_with_small_bar_inputs(oracle, count, seed):
+    """8-word leaves (one Monolith permutation each) whose first concrete
+    layer (round constants zero) outputs values below 2^32 - 1 on lanes 0-3,
+    the lanes that go through the Bars next.  Such a value also has the 64-bit
+    form v + p, and Bars (a byte-wise map, not a field operation) give another
+    result on that form: the input must be canonical.  Solved as
+    M[0..3][0..3] x[0..3] = v - M[0..3][4..7] x[4..7] (mod p)."""
+    P = oracle.P
+    row = _monolith_mds_row()
+    M = [[row[(c - r) % 12] for c in range(12)] for r in range(12)]
+    rng = np.random.default_rng(seed)
+    A = [[M[r][c] for c in range(4)] for r in range(4)]
+
+    def solve(b):  # Gaussian elimination mod p on the 4 x 4 system
+        m = [A[r][:] + [b[r]] for r in range(4)]
+        for col in range(4):
+            piv = next(r for r in range(col, 4) if m[r][col] % P)
+            m[col], m[piv] = m[piv], m[col]
+            inv = pow(m[col][col], P - 2, P)
+            m[col] = [v * inv % P for v in m[col]]
+            for r in range(4):
+                if r != col and m[r][col]:
+                    f = m[r][col]
+                    m[r] = [(a - f * b2) % P for a, b2 in zip(m[r], m[col])]
+        return [m[r][4] for r in range(4)]
+
+    rows = []
+    for _ in range(count):
+        tail = [int(v) for v in rng.integers(0, P, size=4, dtype=np.uint64)]
+        small = [int(v) for v in rng.integers(0, 2**32 - 1, size=4)]
+        rhs = [(small[r] - sum(M[r][4 + k] * tail[k] for k in range(4))) % P for r in range(4)]
+        rows.append(solve(rhs) + tail)
+    return np.array(rows, dtype=np.uint64).reshape(-1)
+
+
+def test_monolith_bars_on_small_values_match_the_cpu_path(zk, oracle):
+    """Regression for a case where zeknox's own GPU build and its CPU path
+    disagree: a concrete-layer output below 2^32 - 1 that reaches the Bars.
+    This library follows the CPU path (and zeknox's known answer): leaf digests
+    equal the oracle's and, when built, zeknox's CPU hash."""
+    nl, ls = 64, 8
+    leaves = _leaves_with_small_bar_inputs(oracle, nl, 0x5EED)
+    d, c = gpu_tree(zk, leaves, ls, 6, 4)  # cap height 6: the cap is the 64 leaf hashes
+    R = oracle.ref()
+    for i in range(nl):
+        row = leaves[i * ls:(i + 1) * ls]
+        want = oracle.hash_one(4, row)
+        assert np.array_equal(c.reshape(-1, 4)[i], want), i
+        if R is not None:
+            ref = np.zeros(4, dtype=np.uint64)
+            R.zkref_hash_one(4, row.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), ls,
+                             ref.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)))
+            assert np.array_equal(ref, want), i
