@@ -486,21 +486,22 @@ def _ev_ms(torch, fn, reps=1):
 
 def run_merkle_only(args):
     """Plain Poseidon Merkle tree, 8192 leaves x 135, cap height 4 (the reference's own CPU-runnable case);
-    --leaves picks another power-of-two leaf count of the same width."""
+    --leaves picks another power-of-two leaf count of the same width, --hash another hasher."""
     import torch
 
     import zeknox_b200 as zk
 
     nl, w, ch = args.leaves, 135, 4
+    ht = HASH_NAMES[args.hash]
     assert nl >= 32 and nl & (nl - 1) == 0, "--leaves must be a power of two >= 32"
     host = field_elems(0x5EED0001, nl * w)
     leaves = torch.from_numpy(host).cuda().view(nl, w)
-    d, c = zk.merkle_tree(leaves, ch, 0)
+    d, c = zk.merkle_tree(leaves, ch, ht)
     for _ in range(args.warmup):
-        zk.merkle_tree(leaves, ch, 0, d, c)
-    ms = _ev_ms(torch, lambda: zk.merkle_tree(leaves, ch, 0, d, c), args.steps)
-    perms = nl * 17 + nl
-    out = {"workload": f"merkle {nl}x135 poseidon cap_height 4", "ms": ms, "perm_per_s": perms / (ms * 1e-3),
+        zk.merkle_tree(leaves, ch, ht, d, c)
+    ms = _ev_ms(torch, lambda: zk.merkle_tree(leaves, ch, ht, d, c), args.steps)
+    perms = nl * ((w + (17 if ht == 1 else 8) - 1) // (17 if ht == 1 else 8)) + nl
+    out = {"workload": f"merkle {nl}x135 {args.hash} cap_height 4", "ms": ms, "perm_per_s": perms / (ms * 1e-3),
            "leaf_elems_per_s": nl * w / (ms * 1e-3)}
     if args.no_cpu_baseline:
         print(json.dumps(out), flush=True)
@@ -509,7 +510,7 @@ def run_merkle_only(args):
 
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
     t0 = time.perf_counter()
-    _, cap_ref = O.ref_merkle_fill(host, w, ch, 0) if O.ref_available() else O.merkle_fill(host, w, ch, 0)
+    _, cap_ref = O.ref_merkle_fill(host, w, ch, ht) if O.ref_available() else O.merkle_fill(host, w, ch, ht)
     out["cpu_reference_ms"] = (time.perf_counter() - t0) * 1e3
     out["cap_equals_cpu_reference"] = bool(np.array_equal(cap_ref.reshape(-1, 4), c.cpu().numpy()))
     print(json.dumps(out), flush=True)

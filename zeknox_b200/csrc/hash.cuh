@@ -493,65 +493,111 @@ constexpr uint64_t kBnNinv = 0xc2e1f593efffffffull;  // -r^-1 mod 2^64
 constexpr uint64_t kBnR2[4] = {0x1bb8e645ae216da7ull, 0x53fe3ab1e35c59e3ull, 0x8c49833d53bb8085ull,
                                0x0216d0b17f4e44a5ull};  // 2^512 mod r
 
-// t - r if t >= r (t < 2r), limb-wise with borrows.
+// t - r if t >= r (t < 2r; `top` is bit 256 of t): one borrow chain.
 __device__ __forceinline__ void bn_reduce_once(uint64_t t[4], uint64_t top) {
-    uint64_t d[4];
-    uint64_t borrow = 0;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const uint64_t ri = bn_r(i) + borrow;
-        const uint64_t b1 = ri < borrow ? 1 : 0;  // r_i + 1 overflowed
-        d[i] = t[i] - ri;
-        borrow = (t[i] < ri ? 1 : 0) | b1;
-    }
-    const bool ge = top || !borrow;
-#pragma unroll
-    for (int i = 0; i < 4; i++) t[i] = ge ? d[i] : t[i];
+    uint64_t d0, d1, d2, d3;
+    uint32_t bw;
+    asm("sub.cc.u64  %0, %5, %9;\n\t"
+        "subc.cc.u64 %1, %6, %10;\n\t"
+        "subc.cc.u64 %2, %7, %11;\n\t"
+        "subc.cc.u64 %3, %8, %12;\n\t"
+        "subc.u32    %4, 0, 0;"
+        : "=l"(d0), "=l"(d1), "=l"(d2), "=l"(d3), "=r"(bw)
+        : "l"(t[0]), "l"(t[1]), "l"(t[2]), "l"(t[3]), "l"(bn_r(0)), "l"(bn_r(1)), "l"(bn_r(2)), "l"(bn_r(3)));
+    const bool ge = top != 0 || bw == 0;
+    t[0] = ge ? d0 : t[0];
+    t[1] = ge ? d1 : t[1];
+    t[2] = ge ? d2 : t[2];
+    t[3] = ge ? d3 : t[3];
 }
+// x + y mod r for x, y < r: one carry chain, then bn_reduce_once.
 __device__ __forceinline__ Fr bn_add(const Fr &x, const Fr &y) {
     Fr z;
-    uint64_t c = 0;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const uint64_t s1 = x.v[i] + y.v[i];
-        const uint64_t c1 = s1 < x.v[i] ? 1 : 0;
-        const uint64_t s2 = s1 + c;
-        c = c1 | (s2 < s1 ? 1 : 0);
-        z.v[i] = s2;
-    }
+    uint32_t c;
+    asm("add.cc.u64  %0, %5, %9;\n\t"
+        "addc.cc.u64 %1, %6, %10;\n\t"
+        "addc.cc.u64 %2, %7, %11;\n\t"
+        "addc.cc.u64 %3, %8, %12;\n\t"
+        "addc.u32    %4, 0, 0;"
+        : "=l"(z.v[0]), "=l"(z.v[1]), "=l"(z.v[2]), "=l"(z.v[3]), "=r"(c)
+        : "l"(x.v[0]), "l"(x.v[1]), "l"(x.v[2]), "l"(x.v[3]), "l"(y.v[0]), "l"(y.v[1]), "l"(y.v[2]), "l"(y.v[3]));
     bn_reduce_once(z.v, c);
     return z;
 }
-// Montgomery product x y / 2^256 mod r (CIOS over 64-bit limbs).
-__device__ __forceinline__ Fr bn_mul(const Fr &x, const Fr &y) {
-    uint64_t t[6] = {0, 0, 0, 0, 0, 0};
+// Montgomery product x y / 2^256 mod r: CIOS over eight 32-bit limbs, each
+// row a pair of carry chains (low halves of the products, then high halves)
+// for t += x y_i and for t += m r, m = t_0 (-r^-1) mod 2^32; the row ends by
+// dropping the zero limb t_0.  t < 2r throughout; one conditional
+// subtraction at the end.
+// Not inlined: a permutation makes ~1050 of these products, and one shared
+// copy of the code keeps the kernel inside the instruction cache (inlined,
+// ncu showed warps waiting on instruction fetch ~3 cycles per issue).
+constexpr uint32_t kBnNinv32 = 0xefffffffu;  // -r^-1 mod 2^32
+__device__ __noinline__ Fr bn_mul(const Fr &x, const Fr &y) {
+    uint32_t a[8], b[8], r[8];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        uint64_t c = 0;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const unsigned __int128 v = (unsigned __int128)x.v[j] * y.v[i] + t[j] + c;
-            t[j] = (uint64_t)v;
-            c = (uint64_t)(v >> 64);
-        }
-        unsigned __int128 v = (unsigned __int128)t[4] + c;
-        t[4] = (uint64_t)v;
-        t[5] = (uint64_t)(v >> 64);
-        const uint64_t m = t[0] * kBnNinv;
-        v = (unsigned __int128)m * bn_r(0) + t[0];
-        c = (uint64_t)(v >> 64);
-#pragma unroll
-        for (int j = 1; j < 4; j++) {
-            v = (unsigned __int128)m * bn_r(j) + t[j] + c;
-            t[j - 1] = (uint64_t)v;
-            c = (uint64_t)(v >> 64);
-        }
-        v = (unsigned __int128)t[4] + c;
-        t[3] = (uint64_t)v;
-        t[4] = t[5] + (uint64_t)(v >> 64);
+        a[2 * i] = (uint32_t)x.v[i];
+        a[2 * i + 1] = (uint32_t)(x.v[i] >> 32);
+        b[2 * i] = (uint32_t)y.v[i];
+        b[2 * i + 1] = (uint32_t)(y.v[i] >> 32);
+        r[2 * i] = (uint32_t)bn_r(i);
+        r[2 * i + 1] = (uint32_t)(bn_r(i) >> 32);
     }
-    Fr z{{t[0], t[1], t[2], t[3]}};
-    bn_reduce_once(z.v, t[4]);
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0, t8 = 0, t9 = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const uint32_t bi = b[i];
+        // t += a * b_i
+        asm("mad.lo.cc.u32  %0, %10, %18, %0;\n\t"
+            "madc.lo.cc.u32 %1, %11, %18, %1;\n\t"
+            "madc.lo.cc.u32 %2, %12, %18, %2;\n\t"
+            "madc.lo.cc.u32 %3, %13, %18, %3;\n\t"
+            "madc.lo.cc.u32 %4, %14, %18, %4;\n\t"
+            "madc.lo.cc.u32 %5, %15, %18, %5;\n\t"
+            "madc.lo.cc.u32 %6, %16, %18, %6;\n\t"
+            "madc.lo.cc.u32 %7, %17, %18, %7;\n\t"
+            "addc.cc.u32    %8, %8, 0;\n\t"
+            "addc.u32       %9, %9, 0;\n\t"
+            "mad.hi.cc.u32  %1, %10, %18, %1;\n\t"
+            "madc.hi.cc.u32 %2, %11, %18, %2;\n\t"
+            "madc.hi.cc.u32 %3, %12, %18, %3;\n\t"
+            "madc.hi.cc.u32 %4, %13, %18, %4;\n\t"
+            "madc.hi.cc.u32 %5, %14, %18, %5;\n\t"
+            "madc.hi.cc.u32 %6, %15, %18, %6;\n\t"
+            "madc.hi.cc.u32 %7, %16, %18, %7;\n\t"
+            "madc.hi.cc.u32 %8, %17, %18, %8;\n\t"
+            "addc.u32       %9, %9, 0;"
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8), "+r"(t9)
+            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(bi));
+        const uint32_t m = t0 * kBnNinv32;
+        // t += m * r (t_0 becomes 0)
+        asm("mad.lo.cc.u32  %0, %10, %18, %0;\n\t"
+            "madc.lo.cc.u32 %1, %11, %18, %1;\n\t"
+            "madc.lo.cc.u32 %2, %12, %18, %2;\n\t"
+            "madc.lo.cc.u32 %3, %13, %18, %3;\n\t"
+            "madc.lo.cc.u32 %4, %14, %18, %4;\n\t"
+            "madc.lo.cc.u32 %5, %15, %18, %5;\n\t"
+            "madc.lo.cc.u32 %6, %16, %18, %6;\n\t"
+            "madc.lo.cc.u32 %7, %17, %18, %7;\n\t"
+            "addc.cc.u32    %8, %8, 0;\n\t"
+            "addc.u32       %9, %9, 0;\n\t"
+            "mad.hi.cc.u32  %1, %10, %18, %1;\n\t"
+            "madc.hi.cc.u32 %2, %11, %18, %2;\n\t"
+            "madc.hi.cc.u32 %3, %12, %18, %3;\n\t"
+            "madc.hi.cc.u32 %4, %13, %18, %4;\n\t"
+            "madc.hi.cc.u32 %5, %14, %18, %5;\n\t"
+            "madc.hi.cc.u32 %6, %15, %18, %6;\n\t"
+            "madc.hi.cc.u32 %7, %16, %18, %7;\n\t"
+            "madc.hi.cc.u32 %8, %17, %18, %8;\n\t"
+            "addc.u32       %9, %9, 0;"
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8), "+r"(t9)
+            : "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(m));
+        t0 = t1, t1 = t2, t2 = t3, t3 = t4, t4 = t5, t5 = t6, t6 = t7, t7 = t8, t8 = t9, t9 = 0;
+    }
+    Fr z{{((uint64_t)t1 << 32) | t0, ((uint64_t)t3 << 32) | t2, ((uint64_t)t5 << 32) | t4,
+          ((uint64_t)t7 << 32) | t6}};
+    bn_reduce_once(z.v, t8);
     return z;
 }
 __device__ __forceinline__ Fr bn_load(const uint64_t (&a)[4]) { return Fr{{a[0], a[1], a[2], a[3]}}; }
