@@ -402,6 +402,11 @@ def main() -> None:
             "peak_source": "INT32 IMAD issue rate measured live by zeknox_b200/libzkprobe.so (MEASURED_PEAKS.json "
                            "has no integer figure)",
             "ms_per_launch": t_mk,
+            # The same kernel against HBM: it reads the leaf matrix once and writes the digests.
+            "hbm_view": {"algorithmic_bytes": B * N * 8 + (nd + nc) * 32,
+                         "achieved_gbs": (B * N * 8 + (nd + nc) * 32) / (t_mk * 1e-3) / 1e9,
+                         "frac": ((B * N * 8 + (nd + nc) * 32) / (t_mk * 1e-3) / 1e9) / hbm_peak if hbm_peak else None,
+                         "note": "integer-issue bound, not memory bound: the fraction of HBM is small by nature"},
         }
         hbm_bytes = LDE_BYTES
         roof_hbm = {
