@@ -87,6 +87,16 @@ def test_host_validation_without_gpu():
     with pytest.raises(zk.ZeknoxError) as e:
         zk.lde_batch(0, 0, 0, 5, cfg)
     assert e.value.code == 1 and "invalid args" in e.value.message
+    # FRI fold: arguments are checked before anything is launched
+    L = zk.capi.LIB
+    assert L.zk_fri_fold_async(None, None, 64, 2, 1, 0, 0, None).code == 1  # null buffers
+    fake = ctypes.c_void_p(16)  # never dereferenced: every call below fails its checks first
+    for n_in, ab, b0, b1 in [(64, 0, 1, 0), (64, 7, 1, 0), (48, 2, 1, 0), (2, 2, 1, 0), (64, 2, 2**64 - 1, 0),
+                             (64, 2, 0, 0xFFFFFFFF00000001)]:
+        err = L.zk_fri_fold_async(fake, ctypes.c_void_p(32), n_in, ab, b0, b1, 0, None)
+        assert err.code == 1, (n_in, ab, b0, b1)
+    assert L.zk_fri_fold_async(fake, fake, 64, 2, 1, 0, 0, None).code == 1  # in place
+    assert L.zk_fri_fold_async(fake, ctypes.c_void_p(40), 64, 2, 1, 0, 1, None).code == 1  # misaligned pairs
     n = zk.get_number_of_gpus()
     assert n >= 0
     if n == 0:  # no device: the calls fail with an error code instead of crashing
