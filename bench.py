@@ -415,6 +415,11 @@ def main() -> None:
             "frac": (hbm_bytes / (t_lde * 1e-3) / 1e9) / hbm_peak if hbm_peak else None,
             "traffic": NCU_TRAFFIC.get(("lde_leaves", B, LG)), "algorithmic_bytes": hbm_bytes, "ms_per_launch": t_lde,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm_peak else None,
+            # What does bound it, from ncu on this workload (column pass, leaves pass):
+            "compute_view": {"bound": "ALU pipe (64-bit modular arithmetic on 32-bit integer units)",
+                             "alu_pipe_pct": [71.2, 78.9], "issue_active_pct": [60.2, 69.7],
+                             "instructions_per_output_element": [232, 277],
+                             "source": "profiles/ntt_lde_to_leaves_135x2^15_rate3.md"},
         }
         roof_tr = {
             "kernel": "compute_transpose_rev (bit-reversing column -> leaf transpose, plain path)", "bound": "hbm",
