@@ -75,6 +75,31 @@ def test_c_header_compiles_as_c_and_matches_layout(tmp_path):
                     str(src), "-o", str(tmp_path / "t2.o")], check=True)
 
 
+def test_c_program_links_and_runs_against_both_libraries(tmp_path):
+    """A C caller (what the Go wrapper's cgo build is) links the shared library
+    alone, or the static archive plus the static CUDA runtime, and calls into
+    it: get_number_of_gpus answers without a device (0 here) or with one."""
+    import shutil
+
+    cuda_lib = Path("/usr/local/cuda/lib64")
+    if not (cuda_lib / "libcudart_static.a").exists() or shutil.which("gcc") is None:
+        pytest.skip("static CUDA runtime or gcc not available")
+    src = tmp_path / "t.c"
+    src.write_text('#include <stdio.h>\n#include <stdlib.h>\n#include "zeknox.h"\n'
+                   "int main(void) {\n  size_t n = 99;\n  RustError e = get_number_of_gpus(&n);\n"
+                   '  printf("%d %zu\\n", e.code, n);\n  free(e.message);\n  return e.code != 0;\n}\n')
+    pkg = ROOT / "zeknox_b200"
+    exe_static, exe_shared = tmp_path / "t_static", tmp_path / "t_shared"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe_static),
+                    str(pkg / "libzeknox.a"), "-L", str(cuda_lib), "-lcudart_static", "-lstdc++", "-ldl", "-lrt",
+                    "-lpthread", "-lm"], check=True)
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe_shared), "-L", str(pkg),
+                    "-lzeknox", f"-Wl,-rpath,{pkg}"], check=True)
+    for exe in (exe_static, exe_shared):
+        out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+        assert out[0] == "0" and int(out[1]) >= 0
+
+
 def test_host_validation_without_gpu():
     import zeknox_b200 as zk
 
