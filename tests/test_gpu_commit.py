@@ -223,3 +223,58 @@ def test_threads_per_hash_tuning_keeps_trees_bit_exact(zk, oracle, lg_n, rate, b
     assert np.array_equal(out.cap.cpu().numpy().reshape(-1), cap)
     assert np.array_equal(out.digests.cpu().numpy().reshape(-1)[:dig.size], dig)
     zk.autotune_reset()
+
+
+def test_drop_in_abi_from_several_host_threads(zk, oracle):
+    """zeknox's Rust tests run concurrently (cargo's test threads): the drop-in
+    calls made from four host threads at once, on host buffers, give the same
+    LDE and caps as the oracle (the per-device streams and tables are shared)."""
+    import threading
+
+    import torch
+
+    shapes = [(9, 2, 20, 2), (10, 3, 7, 3), (8, 1, 33, 1), (11, 2, 3, 4)]  # lg_n, rate, batches, cap height
+    want = []
+    for k, (lg_n, rate, b, ch) in enumerate(shapes):
+        x = oracle.field_elems(7100 + k, b << lg_n)
+        lde = oracle.batch_lde(x, lg_n, rate, b)
+        leaves = oracle.transpose_rev(lde, lg_n + rate, b)
+        _, cap = oracle.merkle_fill(leaves, b, ch, oracle.HASH_POSEIDON)
+        want.append((x, lde, cap))
+    errors = []
+
+    def worker(k):
+        try:
+            torch.cuda.set_device(0)
+            lg_n, rate, b, ch = shapes[k]
+            x, lde_want, cap_want = want[k]
+            N = 1 << (lg_n + rate)
+            nd, nc = 2 * (N - (1 << ch)), 1 << ch
+            for _ in range(3):
+                cfg = zk.NTTConfig.default()
+                cfg.batches, cfg.extension_rate_bits, cfg.with_coset = b, rate, True
+                lde = np.zeros(b * N, dtype=np.uint64)
+                zk.lde_batch(0, lde.ctypes.data, x.ctypes.data, lg_n, cfg)  # host in, host out
+                if not np.array_equal(lde, lde_want):
+                    errors.append((k, "lde"))
+                d_lde = torch.from_numpy(lde).cuda()
+                d_leaves = torch.empty_like(d_lde)
+                tcfg = zk.TransposeConfig.default()
+                tcfg.batches, tcfg.are_inputs_on_device, tcfg.are_outputs_on_device = b, True, True
+                zk.transpose_rev_batch(0, d_leaves.data_ptr(), d_lde.data_ptr(), lg_n + rate, tcfg)
+                dig = torch.zeros(max(nd, 1) * 4, dtype=torch.uint64, device="cuda")
+                cap = torch.zeros(nc * 4, dtype=torch.uint64, device="cuda")
+                zk.fill_digests_buf_linear_gpu_with_gpu_ptr(dig.data_ptr(), cap.data_ptr(), d_leaves.data_ptr(), nd,
+                                                            nc, N, b, ch, zk.HashPoseidon, 0)
+                torch.cuda.synchronize()
+                if not np.array_equal(cap.cpu().numpy(), cap_want):
+                    errors.append((k, "cap"))
+        except Exception as e:  # noqa: BLE001 - reported below
+            errors.append((k, repr(e)))
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(len(shapes))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
