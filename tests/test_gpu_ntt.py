@@ -115,13 +115,20 @@ def test_lde_mixed_host_device(zk, oracle):
     assert np.array_equal(out, exp)
 
 
-def test_lde_salt_rows(zk, oracle):
+@pytest.mark.parametrize("b,out_dev", [(2, False), (33, False), (20, True)])
+def test_lde_salt_rows(zk, oracle, b, out_dev):
     # ntt.cu:541-545: salt_size extra rows of random field elements after the LDE rows
-    lg_n, rate, b, salt = 8, 2, 2, 3
-    x = oracle.field_elems(4, b << lg_n)
+    # (33 and 20 polynomials: salt behind the grouped copy pipeline, host or device output)
+    lg_n, rate, salt = 8, 2, 3
+    x = oracle.field_elems(4 + b, b << lg_n)
     N = 1 << (lg_n + rate)
-    out = np.zeros((b + salt) * N, dtype=np.uint64)
-    zk.lde_batch(0, out.ctypes.data, x.ctypes.data, lg_n, _cfg(zk, b, rate, coset=True, salt=salt))
+    if out_dev:
+        d_out = _dev(np.zeros((b + salt) * N, dtype=np.uint64))
+        zk.lde_batch(0, d_out.data_ptr(), x.ctypes.data, lg_n, _cfg(zk, b, rate, out_dev=True, coset=True, salt=salt))
+        out = _host(d_out)
+    else:
+        out = np.zeros((b + salt) * N, dtype=np.uint64)
+        zk.lde_batch(0, out.ctypes.data, x.ctypes.data, lg_n, _cfg(zk, b, rate, coset=True, salt=salt))
     assert np.array_equal(out[: b * N], oracle.batch_lde(x, lg_n, rate, b))
     s = out[b * N:]
     assert (s < np.uint64(oracle.P)).all() and len(np.unique(s)) > 0.99 * s.size
