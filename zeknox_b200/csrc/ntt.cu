@@ -632,7 +632,7 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
         a.n_valid = j.n_valid;
         if (j.to_leaves) {
             a.to_leaves = 1;
-            a.leaf_stride = j.batches;
+            a.leaf_stride = j.leaf_stride ? j.leaf_stride : j.batches;
             a.lg_t = std::min<uint32_t>(a.lg_t, 4);
         }
         const uint64_t groups = (j.batches + (1ull << a.lg_t) - 1) >> a.lg_t;
@@ -686,7 +686,7 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
                 a.src = scr;
                 a.src_poly_stride = N;
                 a.dst = j.dst + b0;
-                a.leaf_stride = j.batches;
+                a.leaf_stride = j.leaf_stride ? j.leaf_stride : j.batches;
                 a.pre_lo = nullptr;
                 a.n_valid = N;
                 const uint64_t groups = ((nb + (1ull << a.lg_t) - 1) >> a.lg_t) << a.lg_pre;

@@ -31,6 +31,9 @@ struct NttJob {
     // Write the leaf layout instead: element k of polynomial b goes to
     // dst[rev_lg(k) * batches + b] (forward transforms without post_coset/scale).
     bool to_leaves = false;
+    // Words per leaf row when the polynomials are a column slice of a wider
+    // leaf matrix (dst then points at the slice's first column); 0 = batches.
+    uint64_t leaf_stride = 0;
 };
 
 void ntt_run(const NttJob &job, cudaStream_t s);
