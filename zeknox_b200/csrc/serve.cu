@@ -88,6 +88,21 @@ void validate(const Shape &s) {
     require(merkle_hash_supported(s.hash), "unsupported hash type");
 }
 
+// The Merkle forest of a commit's leaves on `st`.
+void forest_on(const Shape &sh, const uint64_t *leaves, uint64_t *digests, uint64_t *cap, cudaStream_t st) {
+    MerkleJob m;
+    m.digests = digests;
+    m.cap = cap;
+    m.leaves = leaves;
+    m.n_digests = sh.n_digests();
+    m.n_caps = sh.n_caps();
+    m.n_leaves = sh.N();
+    m.leaf_size = sh.batches;
+    m.cap_height = sh.cap_h;
+    m.hash_type = sh.hash;
+    merkle_run(m, st);
+}
+
 // The LDE in leaf layout of polynomials [b0, b0 + nb) of a commit: a column
 // slice of the leaf matrix.
 void lde_leaves_slice(DeviceCtx &ctx, const Shape &sh, const uint64_t *coeffs, uint64_t *leaves, uint64_t *scratch,
@@ -139,46 +154,14 @@ void commit_from_host(DeviceCtx &ctx, const Shape &sh, const void *host, uint64_
         throw;
     }
     for (cudaEvent_t e : ev) cudaEventDestroy(e);
-    MerkleJob m;
-    m.digests = digests;
-    m.cap = cap;
-    m.leaves = leaves;
-    m.n_digests = sh.n_digests();
-    m.n_caps = sh.n_caps();
-    m.n_leaves = sh.N();
-    m.leaf_size = sh.batches;
-    m.cap_height = sh.cap_h;
-    m.hash_type = sh.hash;
-    merkle_run(m, st);
+    forest_on(sh, leaves, digests, cap, st);
 }
 
 // One commit on `st`: LDE in leaf layout (scratch supplied), then the forest.
 void commit_on(DeviceCtx &ctx, const Shape &sh, const uint64_t *coeffs, uint64_t *leaves, uint64_t *digests,
                uint64_t *cap, uint64_t *scratch, cudaStream_t st) {
-    const uint32_t lg = sh.lg_n + sh.rate;
-    NttJob j;
-    j.src = coeffs;
-    j.src_stride = sh.n();
-    j.n_valid = sh.n();
-    j.dst = leaves;
-    j.batches = sh.batches;
-    j.lg = lg;
-    j.pre_coset = &coset_table(ctx, lg, GROUP_GENERATOR, false);
-    j.to_leaves = true;
-    j.scratch = scratch;
-    j.scratch_elems = ntt_scratch_elems(lg, sh.batches);
-    ntt_run(j, st);
-    MerkleJob m;
-    m.digests = digests;
-    m.cap = cap;
-    m.leaves = leaves;
-    m.n_digests = sh.n_digests();
-    m.n_caps = sh.n_caps();
-    m.n_leaves = sh.N();
-    m.leaf_size = sh.batches;
-    m.cap_height = sh.cap_h;
-    m.hash_type = sh.hash;
-    merkle_run(m, st);
+    lde_leaves_slice(ctx, sh, coeffs, leaves, scratch, 0, sh.batches, st);
+    forest_on(sh, leaves, digests, cap, st);
 }
 
 // Per-device pool of internal streams for batches.
