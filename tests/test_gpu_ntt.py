@@ -263,3 +263,27 @@ def test_transpose_vs_zeknox_sm100_build(zk, oracle):
     assert R.compute_transpose_rev(0, ref_out.ctypes.data, x.ctypes.data, lg, c).code == 0
     zk.transpose_rev_batch(0, out.ctypes.data, x.ctypes.data, lg, c)
     assert np.array_equal(out, ref_out)
+
+
+def test_empty_inputs_are_no_ops(zk):
+    """Zero polynomials (and zero jobs / queries for the extensions) are valid
+    calls that do nothing: null buffers are accepted, nothing is launched."""
+    import torch
+
+    before = zk.capi.LIB.zk_kernel_launches()
+    cfg = _cfg(zk, 0, 0)
+    zk.ntt_batch(0, 0, 10, cfg)
+    zk.intt_batch(0, 0, 10, cfg)
+    zk.lde_batch(0, 0, 0, 10, _cfg(zk, 0, 2, coset=True))
+    zk.lde_batch(0, 0, 0, 10, _cfg(zk, 0, 2, in_dev=True, out_dev=True, coset=True))
+    tcfg = zk.TransposeConfig.default()
+    tcfg.batches, tcfg.are_inputs_on_device, tcfg.are_outputs_on_device = 0, True, True
+    zk.transpose_rev_batch(0, 0, 0, 10, tcfg)
+    zk.capi.check(zk.capi.LIB.zk_commit_batch(None, 0, 4, None))
+    leaves = torch.zeros((16, 4), dtype=torch.uint64, device="cuda")
+    digests, _ = zk.merkle_tree(leaves, 2, 0)
+    rows, sib = zk.merkle_open(leaves, digests, 2, torch.zeros(0, dtype=torch.int64))
+    torch.cuda.synchronize()
+    assert rows.shape == (0, 4) and sib.shape[0] == 0
+    # only the tree above launched kernels
+    assert zk.capi.LIB.zk_kernel_launches() - before <= 8
