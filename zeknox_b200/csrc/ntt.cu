@@ -107,11 +107,18 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // order 192 and the 8th roots are powers of 2: for omega_8 = 7^((p-1)/8)
 // (the root every table here is built from), omega_8 = 2^120 = -2^24,
 // omega_8^2 = omega_4 = 2^48, omega_8^3 = -2^72, and the inverses are 2^72,
-// -2^48, 2^24.  x * 2^24 and x * 2^48 are a shift and one reduction, not a
-// 64 x 64 product; 2^72 stays a product with a constant.
-constexpr uint64_t kTwo72 = 0xffffffff00ull;  // 2^72 mod p = 2^40 - 2^8
+// -2^48, 2^24.  None of the three is a 64 x 64 product: x * 2^24 and x * 2^48
+// are a shift and one reduction, x * 2^72 is two shifts and a subtraction.
 __device__ __forceinline__ uint64_t gl_mul2_24(uint64_t x) { return gl_reduce96(x << 24, (uint32_t)(x >> 40)); }
 __device__ __forceinline__ uint64_t gl_mul2_48(uint64_t x) { return gl_reduce128(x << 48, x >> 16); }
+// x * 2^72 for canonical x: with x = xh 2^24 + xl (xl < 2^24), 2^96 = -1 gives
+// x 2^72 = xl 2^72 - xh = xl (2^40 - 2^8) - xh (mod p), where
+// xl (2^40 - 2^8) < p and xh < 2^40; one correction on borrow keeps it canonical.
+__device__ __forceinline__ uint64_t gl_mul2_72(uint64_t x) {
+    const uint64_t xl = x & 0xffffffull, xh = x >> 24;
+    const uint64_t a = (xl << 40) - (xl << 8);
+    return a >= xh ? a - xh : a - xh - ZK_EPS;  // on borrow, 2^64 - eps = p is added back
+}
 
 // 8-point DFT in place (DIF radix-2 inside, natural order in, bit-reversed
 // out), with the direction's 8th roots.  Negated roots swap the operands of
@@ -122,9 +129,9 @@ __device__ __forceinline__ void dft8(uint64_t x[8], bool inv) {
     if (!inv) {
         d[1] = gl_mul2_24(gl_sub(x[5], x[1]));      // (x1 - x5) * (-2^24)
         d[2] = gl_mul2_48(gl_sub(x[2], x[6]));      // (x2 - x6) * 2^48
-        d[3] = gl_mul(gl_sub(x[7], x[3]), kTwo72);  // (x3 - x7) * (-2^72)
+        d[3] = gl_mul2_72(gl_sub(x[7], x[3]));      // (x3 - x7) * (-2^72)
     } else {
-        d[1] = gl_mul(gl_sub(x[1], x[5]), kTwo72);  // * 2^72
+        d[1] = gl_mul2_72(gl_sub(x[1], x[5]));      // * 2^72
         d[2] = gl_mul2_48(gl_sub(x[6], x[2]));      // * (-2^48)
         d[3] = gl_mul2_24(gl_sub(x[3], x[7]));      // * 2^24
     }
