@@ -7,7 +7,9 @@ device buffers:
   fill_digests_buf_linear_gpu_with_gpu_ptr, every output compared word for
   word (LDE matrix, leaves, digests, cap);
 * the hash sweep's trees (2^20 leaves x 135, cap 4) for Poseidon, Poseidon2,
-  Keccak and Monolith, and a 2^16-leaf tree for Poseidon-BN128, digests and
+  Keccak and Monolith, a 2^16-leaf tree for Poseidon-BN128, and the
+  8192-leaf tree of the CPU-runnable Merkle case (8192 x 135, cap 4) for the
+  four Goldilocks hashers, digests and
   cap compared (Monolith against zeknox's CPU build: its GPU build differs
   from its own CPU path on rare inputs, see the Monolith test in
   test_gpu_merkle.py).
@@ -126,7 +128,7 @@ def test_default_commit_equals_and_outruns_the_reference_build(zk, ref, oracle):
     assert times["ours"]["total_ms"] <= times["reference"]["total_ms"], entry
 
 
-@pytest.mark.parametrize("ht,lg_leaves", [(0, 20), (3, 20), (1, 20), (4, 20), (2, 16)])
+@pytest.mark.parametrize("ht,lg_leaves", [(0, 20), (3, 20), (1, 20), (4, 20), (2, 16), (0, 13), (3, 13), (1, 13), (4, 13)])
 def test_sweep_trees_equal_and_outrun_the_reference_build(zk, ref, oracle, ht, lg_leaves):
     import torch
 
@@ -139,7 +141,8 @@ def test_sweep_trees_equal_and_outrun_the_reference_build(zk, ref, oracle, ht, l
                        ("ours", zk.capi.LIB.fill_digests_buf_linear_gpu_with_gpu_ptr)):
         dig = torch.zeros(nd * 4, dtype=torch.uint64, device="cuda")
         cap = torch.zeros(nc * 4, dtype=torch.uint64, device="cuda")
-        t = _timed(lambda: fill(dig.data_ptr(), cap.data_ptr(), leaves.data_ptr(), nd, nc, nl, w, ch, ht, 0), reps=2)
+        t = _timed(lambda: fill(dig.data_ptr(), cap.data_ptr(), leaves.data_ptr(), nd, nc, nl, w, ch, ht, 0),
+                   reps=2 if lg_leaves >= 16 else 10)
         res[name] = (t, dig, cap)
     entry = {"case": f"merkle 2^{lg_leaves} x 135, cap 4, hash type {ht}", "reference_ms": res["reference"][0],
              "ours_ms": res["ours"][0], "speedup": res["reference"][0] / res["ours"][0]}
