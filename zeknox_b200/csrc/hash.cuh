@@ -16,6 +16,8 @@
 #pragma once
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "gl64.cuh"
 #include "zk_constants.h"
 
@@ -904,16 +906,23 @@ __device__ __forceinline__ void poseidon_hash_one_duo(const uint64_t *in, uint32
 // row pair (t, t + 6) of the split above: rows of A + B and A - B held in
 // registers.  About a third of the single-thread path's instructions per
 // thread, so about a third of its latency.
-struct HexGroup {
+struct HexLanes {
     uint32_t t;     // thread within the group, 0..5 (lanes 30, 31: 0..1 of a dummy group)
     uint32_t base;  // warp lane of the group's thread 0
-    double p2[6], q2[6];  // row t of A + B and A - B (with the diagonal term on row 0)
-    double fix6;          // -2 d on thread 0 (lane 6 must not get the diagonal), else 0
-    __device__ __forceinline__ HexGroup() {
+    __device__ __forceinline__ HexLanes() {
         const uint32_t lane = threadIdx.x & 31;
         const uint32_t g = lane < 30 ? lane / 6 : 0;
         t = lane < 30 ? lane % 6 : lane - 30;
         base = 6 * g;
+    }
+    // true for the lanes whose group is a real one (not lanes 30, 31)
+    __device__ __forceinline__ bool real() const { return (threadIdx.x & 31) < 30; }
+    __device__ __forceinline__ uint32_t group_in_warp() const { return base / 6; }
+};
+struct HexGroup : HexLanes {
+    double p2[6], q2[6];  // row t of A + B and A - B (with the diagonal term on row 0)
+    double fix6;          // -2 d on thread 0 (lane 6 must not get the diagonal), else 0
+    __device__ __forceinline__ explicit HexGroup(const PoseidonTab &) : HexLanes() {
 #pragma unroll
         for (int k = 0; k < 6; k++) {
             p2[k] = (double)mds_p2((int)t, k);
@@ -921,9 +930,6 @@ struct HexGroup {
         }
         fix6 = t == 0 ? -2.0 * (double)mds_diag0() : 0.0;
     }
-    // true for the lanes whose group is a real one (not lanes 30, 31)
-    __device__ __forceinline__ bool real() const { return (threadIdx.x & 31) < 30; }
-    __device__ __forceinline__ uint32_t group_in_warp() const { return base / 6; }
 };
 
 __device__ __forceinline__ uint64_t shfl64(uint64_t v, uint32_t src) {
@@ -976,22 +982,168 @@ __device__ __forceinline__ void poseidon_permute_hex(uint64_t &o0, uint64_t &o1,
     }
 }
 
+// ------------------------------------------- Poseidon2 on six threads
+// The same group layout: thread t owns state lanes t and t + 6.
+//
+// External layer: output lane r is sum_b (1 + [b == r / 4]) (M4 x_b)[r % 4]
+// over the three 4-lane blocks x_b.  Row c + 2 of M4 is row c rotated by two
+// columns (M4[c + 2][d] = M4[c][d + 2], indices mod 4), and lane t + 6 has
+// column (t + 2) % 4, so thread t needs only m = M4[t % 4]: lane t takes
+// x_(4b + d) with m[d], lane t + 6 with m[(d + 2) % 4], and each lane weighs
+// the three block sums by w in {1, 2}.  As in the one-thread layer, each
+// 32-bit half runs in exact FP64 (every sum below 2^39), offset by 2^52.
+//
+// Internal layer (x_i <- x_i D_i + sum_j x_j + c_i): each thread adds its
+// two lanes exactly (65 bits), the group all-gathers the six partial sums
+// (96-bit total), and each thread forms its two lanes' products.
+struct HexGroup2 : HexLanes {
+    double m[4];          // row t % 4 of M4
+    double w0[3], w1[3];  // block weights of lanes t and t + 6
+    uint64_t d0, d1;      // internal diagonal of lanes t and t + 6
+    __device__ __forceinline__ explicit HexGroup2(const Poseidon2Tab &tab) : HexLanes() {
+        // M4 rows 0 and 1; rows 2 and 3 are these rotated by two columns.
+        const uint32_t c = t & 3, r = c & 1, rot = c & 2;
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            const uint32_t k = (d + rot) & 3;
+            const double row0 = k == 0 ? 5.0 : k == 1 ? 7.0 : k == 2 ? 1.0 : 3.0;
+            const double row1 = k == 0 ? 4.0 : k == 1 ? 6.0 : 1.0;
+            m[d] = r ? row1 : row0;
+        }
+#pragma unroll
+        for (uint32_t b = 0; b < 3; b++) {
+            w0[b] = b == t / 4 ? 2.0 : 1.0;
+            w1[b] = b == (t + 6) / 4 ? 2.0 : 1.0;
+        }
+        d0 = tab.diag[t];
+        d1 = tab.diag[t + 6];
+    }
+};
+
+// External layer on a group, plus the constants cm (adjusted for the magic
+// offsets; nullptr: none).
+__device__ __forceinline__ void poseidon2_external_hex(uint64_t &o0, uint64_t &o1, const HexGroup2 &g,
+                                                       const uint64_t *cm) {
+    uint64_t x[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) x[i] = shfl64(i < 6 ? o0 : o1, g.base + (i % 6));
+    double first[2], second[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        double v[12];
+#pragma unroll
+        for (int i = 0; i < 12; i++) v[i] = magic_in(h ? (uint32_t)(x[i] >> 32) : (uint32_t)x[i]) - kMagic;
+        double a0 = kMagic, a1 = kMagic;
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            double y0 = g.m[0] * v[4 * b], y1 = g.m[2] * v[4 * b];
+#pragma unroll
+            for (int d = 1; d < 4; d++) {
+                y0 = fma(g.m[d], v[4 * b + d], y0);
+                y1 = fma(g.m[(d + 2) & 3], v[4 * b + d], y1);
+            }
+            a0 = fma(g.w0[b], y0, a0);
+            a1 = fma(g.w1[b], y1, a1);
+        }
+        first[h] = a0;
+        second[h] = a1;
+    }
+    o0 = pr_reduce_split(magic_out(first[0]), magic_out(first[1]), cm ? cm[g.t] : kMagicNeg);
+    o1 = pr_reduce_split(magic_out(second[0]), magic_out(second[1]), cm ? cm[g.t + 6] : kMagicNeg);
+}
+
+// Internal layer on a group, plus the next round's constants c (unadjusted).
+__device__ __forceinline__ void poseidon2_internal_hex(uint64_t &o0, uint64_t &o1, const HexGroup2 &g,
+                                                       const uint64_t *c) {
+    uint32_t p0, p1, p2;
+    asm("add.cc.u32 %0, %3, %5;\n\t"
+        "addc.cc.u32 %1, %4, %6;\n\t"
+        "addc.u32 %2, 0, 0;"
+        : "=r"(p0), "=r"(p1), "=r"(p2)
+        : "r"((uint32_t)o0), "r"((uint32_t)(o0 >> 32)), "r"((uint32_t)o1), "r"((uint32_t)(o1 >> 32)));
+    uint32_t s0 = 0, s1 = 0, s2 = 0;  // sum of the 12 lanes, below 12 * 2^64
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        const uint32_t src = g.base + k;
+        const uint32_t q0 = (uint32_t)__shfl_sync(0xffffffffu, (int)p0, (int)src);
+        const uint32_t q1 = (uint32_t)__shfl_sync(0xffffffffu, (int)p1, (int)src);
+        const uint32_t q2 = (uint32_t)__shfl_sync(0xffffffffu, (int)p2, (int)src);
+        asm("add.cc.u32 %0, %0, %3;\n\t"
+            "addc.cc.u32 %1, %1, %4;\n\t"
+            "addc.u32 %2, %2, %5;"
+            : "+r"(s0), "+r"(s1), "+r"(s2)
+            : "r"(q0), "r"(q1), "r"(q2));
+    }
+    uint64_t lane[2] = {o0, o1};
+    const uint64_t cc[2] = {c[g.t], c[g.t + 6]};
+    const uint64_t dd[2] = {g.d0, g.d1};
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        uint32_t c0, c1, c2;
+        asm("add.cc.u32 %0, %3, %6;\n\t"
+            "addc.cc.u32 %1, %4, %7;\n\t"
+            "addc.u32 %2, %5, 0;"
+            : "=r"(c0), "=r"(c1), "=r"(c2)
+            : "r"(s0), "r"(s1), "r"(s2), "r"((uint32_t)cc[j]), "r"((uint32_t)(cc[j] >> 32)));
+        lane[j] = pr_mul_add(lane[j], dd[j], ((uint64_t)c1 << 32) | c0, c2);
+    }
+    o0 = lane[0];
+    o1 = lane[1];
+}
+
+// The rounds of poseidon2_permute on a group.
+__device__ __forceinline__ void poseidon2_permute_hex(uint64_t &o0, uint64_t &o1, const HexGroup2 &g,
+                                                      const Poseidon2Tab &tab) {
+    poseidon2_external_hex(o0, o1, g, &tab.rcm.v[0]);
+#pragma unroll 1
+    for (int rnd = 0; rnd < 4; rnd++) {
+        o0 = pr_pow7(o0);
+        o1 = pr_pow7(o1);
+        poseidon2_external_hex(o0, o1, g, &tab.rcm.v[12 * (rnd + 1)]);
+    }
+#pragma unroll 1
+    for (int rnd = 4; rnd < 26; rnd++) {
+        const uint64_t y = pr_pow7(o0);
+        if (g.t == 0) o0 = y;
+        poseidon2_internal_hex(o0, o1, g, &tab.rc.v[12 * (rnd + 1)]);
+    }
+#pragma unroll 1
+    for (int rnd = 26; rnd < 30; rnd++) {
+        o0 = pr_pow7(o0);
+        o1 = pr_pow7(o1);
+        poseidon2_external_hex(o0, o1, g, rnd < 29 ? &tab.rcm.v[12 * (rnd + 1)] : nullptr);
+    }
+}
+
+__device__ __forceinline__ void permute_hex(uint64_t &o0, uint64_t &o1, const HexGroup &g, const PoseidonTab &tab) {
+    poseidon_permute_hex(o0, o1, g, tab);
+}
+__device__ __forceinline__ void permute_hex(uint64_t &o0, uint64_t &o1, const HexGroup2 &g, const Poseidon2Tab &tab) {
+    poseidon2_permute_hex(o0, o1, g, tab);
+}
+
+// The group form of a hasher: HexOf<kPoseidon> or HexOf<kPoseidon2>.
+template <int H>
+using HexOf = typename std::conditional<H == kPoseidon, HexGroup, HexGroup2>::type;
+
 // H(l || r) on a group: every lane calls; `active` groups load and store.
-__device__ __forceinline__ void poseidon_hash_two_hex(const uint64_t *l, const uint64_t *r, uint64_t *out,
-                                                      bool active, const HexGroup &g, const PoseidonTab &tab) {
+template <class G, class Tab>
+__device__ __forceinline__ void hash_two_hex(const uint64_t *l, const uint64_t *r, uint64_t *out, bool active,
+                                             const G &g, const Tab &tab) {
     uint64_t o0 = 0, o1 = 0;
     if (active) {
         o0 = gl_canon(g.t < 4 ? l[g.t] : r[g.t - 4]);
         if (g.t < 2) o1 = gl_canon(r[g.t + 2]);
     }
-    poseidon_permute_hex(o0, o1, g, tab);
+    permute_hex(o0, o1, g, tab);
     if (active && g.t < 4) out[g.t] = gl_canon(o0);
 }
 
 // Sponge of n words (zeknox's hash_or_noop: n <= 4 copies and zero-pads).
 // n must be the same for all groups of a warp.
-__device__ __forceinline__ void poseidon_hash_one_hex(const uint64_t *in, uint32_t n, uint64_t *out, bool active,
-                                                      const HexGroup &g, const PoseidonTab &tab) {
+template <class G, class Tab>
+__device__ __forceinline__ void hash_one_hex(const uint64_t *in, uint32_t n, uint64_t *out, bool active, const G &g,
+                                             const Tab &tab) {
     if (n <= 4) {
         if (active && g.t < 4) out[g.t] = g.t < n ? in[g.t] : 0ull;
         return;
@@ -1003,7 +1155,7 @@ __device__ __forceinline__ void poseidon_hash_one_hex(const uint64_t *in, uint32
             if (g.t < len) o0 = gl_canon(in[idx + g.t]);
             if (g.t + 6 < len) o1 = gl_canon(in[idx + g.t + 6]);
         }
-        poseidon_permute_hex(o0, o1, g, tab);
+        permute_hex(o0, o1, g, tab);
     }
     if (active && g.t < 4) out[g.t] = gl_canon(o0);
 }

@@ -4,9 +4,10 @@
 // One launch hashes every leaf (one thread per leaf, sponge state in
 // registers), then one launch per tree level hashes that level's nodes across
 // all subtrees, and a last one the narrow top and the cap: the structure of
-// zeknox's kernels (merkle.cu:215-243).  For Poseidon, the latency-bound
-// parts (small trees, narrow levels, the top) spread each permutation over
-// six or two threads instead (hash.cuh), with thresholds set by measurement.
+// zeknox's kernels (merkle.cu:215-243).  For Poseidon and Poseidon2, the
+// latency-bound parts (small trees, narrow levels, the top) spread each
+// permutation over six threads (Poseidon also over two) instead (hash.cuh),
+// with thresholds set by measurement.
 // Fusing the lower levels into the leaf kernel (a block folding its tile of
 // leaves through shared memory) measured slower on B200: a block then holds
 // its registers through the serial, mostly idle fold levels, which costs more
@@ -132,31 +133,34 @@ __global__ void __launch_bounds__(kDuoThreads) merkle_leaves_duo(const uint64_t 
     pdl_release();
 }
 
-// Poseidon on six threads per hash (HexGroup): five hashes per warp.  For the
-// latency-bound cases: few leaves, narrow levels, the top of the tree.
+// Poseidon and Poseidon2 on six threads per hash (HexGroup, HexGroup2): five
+// hashes per warp.  For the latency-bound cases: few leaves, narrow levels,
+// the top of the tree.
 constexpr int kHexThreads = 128;  // 4 warps = 20 hashes per block
 constexpr uint64_t kHexPerBlock = 20;
 
+template <int H>
 __global__ void __launch_bounds__(kHexThreads) merkle_leaves_hex(const uint64_t *__restrict__ leaves,
                                                                  uint64_t n_leaves, uint32_t leaf_size,
                                                                  uint64_t *__restrict__ out, LeafMap map) {
-    __shared__ PoseidonTab tab;
-    load_tab<kPoseidon>(tab);
-    const HexGroup g;
+    __shared__ typename TabOf<H>::type tab;
+    load_tab<H>(tab);
+    const HexOf<H> g(tab);
     const uint64_t first = ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5) * 5;
     if (first >= n_leaves) return;  // whole warp
     const uint64_t i = first + g.group_in_warp();
     const bool active = g.real() && i < n_leaves;
     const uint64_t ii = active ? i : 0;
-    poseidon_hash_one_hex(leaves + ii * leaf_size, leaf_size, out + 4 * map.slot(ii), active, g, tab);
+    hash_one_hex(leaves + ii * leaf_size, leaf_size, out + 4 * map.slot(ii), active, g, tab);
     pdl_release();
 }
 
+template <int H>
 __global__ void __launch_bounds__(kHexThreads) merkle_level_hex(uint64_t *__restrict__ digests, uint32_t lg_w,
                                                                 uint64_t n_caps, uint64_t ds) {
-    __shared__ PoseidonTab tab;
-    load_tab<kPoseidon>(tab);
-    const HexGroup g;
+    __shared__ typename TabOf<H>::type tab;
+    load_tab<H>(tab);
+    const HexOf<H> g(tab);
     const uint64_t w = 1ull << lg_w;
     const uint64_t first = ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5) * 5;
     if (first >= (n_caps << lg_w)) return;  // whole warp
@@ -166,16 +170,17 @@ __global__ void __launch_bounds__(kHexThreads) merkle_level_hex(uint64_t *__rest
     const uint64_t sub = tt >> lg_w, i = (w - 2) + (tt & (w - 1));
     uint64_t *base = digests + 4 * sub * ds;
     pdl_wait();
-    poseidon_hash_two_hex(base + 4 * (2 * i + 2), base + 4 * (2 * i + 3), base + 4 * i, active, g, tab);
+    hash_two_hex(base + 4 * (2 * i + 2), base + 4 * (2 * i + 3), base + 4 * i, active, g, tab);
     pdl_release();
 }
 
 // One block per subtree: levels of width w_top (<= 32) .. 1, then the cap.
+template <int H>
 __global__ void __launch_bounds__(224) merkle_top_hex(uint64_t *__restrict__ digests, uint64_t *__restrict__ cap,
                                                        uint64_t ds, uint32_t w_top) {
-    __shared__ PoseidonTab tab;
-    load_tab<kPoseidon>(tab);
-    const HexGroup g;
+    __shared__ typename TabOf<H>::type tab;
+    load_tab<H>(tab);
+    const HexOf<H> g(tab);
     const uint64_t sub = blockIdx.x;
     uint64_t *base = digests + 4 * sub * ds;
     const uint32_t node = (threadIdx.x >> 5) * 5 + g.group_in_warp();
@@ -186,7 +191,7 @@ __global__ void __launch_bounds__(224) merkle_top_hex(uint64_t *__restrict__ dig
             const uint32_t i = active ? node : 0;
             const uint64_t *c = base + 4 * (2 * w - 2 + 2 * i);  // children 2i, 2i+1 of the level of width 2w
             uint64_t *o = w >= 2 ? base + 4 * (w - 2 + i) : cap + 4 * sub;
-            poseidon_hash_two_hex(c, c + 4, o, active, g, tab);
+            hash_two_hex(c, c + 4, o, active, g, tab);
         }
         __syncthreads();
     }
@@ -232,7 +237,7 @@ uint8_t leaf_layout(uint64_t n_leaves, uint64_t leaf_size) {
 void launch_poseidon_leaves(const uint64_t *leaves, uint64_t n_leaves, uint32_t w, uint64_t *out, LeafMap map,
                             uint8_t layout, cudaStream_t st) {
     if (layout == 6)
-        merkle_leaves_hex<<<hex_blocks(n_leaves), kHexThreads, 0, st>>>(leaves, n_leaves, w, out, map);
+        merkle_leaves_hex<kPoseidon><<<hex_blocks(n_leaves), kHexThreads, 0, st>>>(leaves, n_leaves, w, out, map);
     else if (layout == 2)
         merkle_leaves_duo<<<blocks_for(2 * n_leaves, kDuoThreads), kDuoThreads, 0, st>>>(leaves, n_leaves, w, out, map);
     else
@@ -264,29 +269,44 @@ void merkle_run_t(const MerkleJob &j, cudaStream_t st) {
     map.direct = (ls == 2);
     map.lg_ls = (uint32_t)__builtin_ctzll(ls);
     map.ds = ds;
-    if constexpr (H == kPoseidon) {
+    if constexpr (H == kPoseidon || H == kPoseidon2) {
         // Latency-bound parts on several threads per hash: the leaves of
-        // small trees (leaf_layout), levels of fewer than kHexNodes nodes,
+        // small trees (leaf_layout for Poseidon; Poseidon2 has the six-thread
+        // form only, up to kHexLeaves), levels of fewer than kHexNodes nodes,
         // and the top (<= 32 nodes per subtree, so that one SM per subtree
         // stays latency- rather than issue-bound) in one launch.  Measured
-        // per level: 16384 nodes 46 us six-threaded vs 40 us one-threaded
-        // (issue bound: six threads do twice the instructions of one); 4096
-        // nodes 20 us vs 40 us.
+        // per Poseidon level: 16384 nodes 46 us six-threaded vs 40 us
+        // one-threaded (issue bound: six threads do twice the instructions of
+        // one); 4096 nodes 20 us vs 40 us.
         constexpr uint64_t kHexNodes = 1 << 14;
-        launch_poseidon_leaves(j.leaves, j.n_leaves, w, j.digests, map, leaf_layout(j.n_leaves, w), st);
+        if constexpr (H == kPoseidon) {
+            launch_poseidon_leaves(j.leaves, j.n_leaves, w, j.digests, map, leaf_layout(j.n_leaves, w), st);
+        } else {
+            if (j.n_leaves <= kHexLeaves)
+                merkle_leaves_hex<H><<<hex_blocks(j.n_leaves), kHexThreads, 0, st>>>(j.leaves, j.n_leaves, w,
+                                                                                     j.digests, map);
+            else
+                merkle_leaves<H><<<blocks_for(j.n_leaves, kLeafThreads), kLeafThreads, 0, st>>>(j.leaves, j.n_leaves,
+                                                                                                 w, j.digests, map);
+            ZK_CHECK_LAUNCH();
+        }
         uint32_t lg_top = 0;
         while (lg_top + 1 < map.lg_ls && lg_top < 5 && (j.n_caps << (lg_top + 1)) < kHexNodes) lg_top++;
+        // Wide levels: the 12-lane S-box for Poseidon (measured 15 us faster
+        // per tree of 2^18), the 4-lane one for Poseidon2 (as in its leaves).
+        constexpr int kWideW = H == kPoseidon ? 12 : 4;
         for (uint32_t lg_w = map.lg_ls - 1; lg_w > lg_top; lg_w--) {
             const uint64_t nodes = j.n_caps << lg_w;
-            if (nodes >= kHexNodes)  // 12-lane S-box, as in the leaves (measured 15 us faster per tree of 2^18)
-                launch_after(merkle_level<H, 12>, blocks_for(nodes, kLeafThreads), kLeafThreads, 0, st, j.digests,
+            if (nodes >= kHexNodes)
+                launch_after(merkle_level<H, kWideW>, blocks_for(nodes, kLeafThreads), kLeafThreads, 0, st, j.digests,
                              lg_w, j.n_caps, ds);
             else
-                launch_after(merkle_level_hex, hex_blocks(nodes), kHexThreads, 0, st, j.digests, lg_w, j.n_caps, ds);
+                launch_after(merkle_level_hex<H>, hex_blocks(nodes), kHexThreads, 0, st, j.digests, lg_w, j.n_caps,
+                             ds);
         }
         require(j.n_caps < (1ull << 31), "too many subtrees");
         const uint32_t w_top = 1u << lg_top;
-        launch_after(merkle_top_hex, (unsigned)j.n_caps, 32 * ((w_top + 4) / 5), 0, st, j.digests, j.cap, ds,
+        launch_after(merkle_top_hex<H>, (unsigned)j.n_caps, 32 * ((w_top + 4) / 5), 0, st, j.digests, j.cap, ds,
                      w_top);
         return;
     }

@@ -83,13 +83,8 @@ __device__ __forceinline__ uint32_t brev_bits(uint32_t x, uint32_t bits) {
     return bits ? (__brev(x) >> (32 - bits)) : 0u;
 }
 
-// DIF butterfly (u, v) -> (u + v, (u - v) w).
-__device__ __forceinline__ void bfly(uint64_t &u, uint64_t &v, uint64_t w) {
-    const uint64_t d = gl_sub(u, v);
-    u = gl_add(u, v);
-    v = gl_mul(d, w);
-}
-__device__ __forceinline__ void bfly1(uint64_t &u, uint64_t &v) {  // w = 1
+// DIF butterfly with w = 1: (u, v) -> (u + v, u - v).
+__device__ __forceinline__ void bfly1(uint64_t &u, uint64_t &v) {
     const uint64_t d = gl_sub(u, v);
     u = gl_add(u, v);
     v = d;
