@@ -101,7 +101,12 @@ def test_vs_reference_cpu_fixtures(zk, oracle, golden):
 @pytest.mark.parametrize("ht", [0, 3, 1, 4, 2])
 @pytest.mark.parametrize("nl,ls,ch", [(4096, 135, 4), (2048, 8, 0), (1024, 17, 10), (8192, 5, 3), (64, 200, 5),
                                      (1 << 16, 24, 0), (1 << 16, 9, 6), (1 << 15, 12, 12), (1 << 14, 135, 4),
-                                     (1 << 14, 3, 2), (1 << 14, 13, 14)])
+                                     (1 << 14, 3, 2), (1 << 14, 13, 14),
+                                     # wrappers/rust/tests/merkle_tree.rs:161-223 (4096 x 7, cap 1); the
+                                     # hand-built 4-leaf trees of native/tests/tests.cu:338-375; short
+                                     # leaves (no permutation) on the small-tree kernels; cap == leaves
+                                     (4096, 7, 1), (4, 7, 0), (4, 7, 1), (2, 9, 0), (8192, 4, 2),
+                                     (8192, 1, 0), (1 << 13, 135, 13)])
 def test_vs_oracle(zk, oracle, ht, nl, ls, ch):
     leaves = oracle.field_elems(ht * 1000 + nl + ls, nl * ls)
     d, c = gpu_tree(zk, leaves, ls, ch, ht)
