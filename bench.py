@@ -34,10 +34,16 @@ METRIC = "Goldilocks LDE+Merkle commit elems/s, batched vs plain, bit-exact; p99
 P = 0xFFFFFFFF00000001
 HASH_NAMES = {"poseidon": 0, "keccak": 1, "poseidonbn128": 2, "poseidon2": 3, "monolith": 4}
 # INT32 multiply-class ops per permutation (a 64x64 mulmod counts 10, a
-# small-constant MAC 4): Poseidon 1077 mulmod + 1152 MAC, Poseidon2 736 mulmod,
-# Keccak-f 3720 64-bit logic ops counted as 2 each, Monolith 66 mulmod (bricks)
-# + 1008 MAC (7 concrete layers).
-OPS_PER_PERM = {0: 15378, 3: 7360, 1: 7440, 4: 4692}
+# small-constant MAC 4): Poseidon 1077 mulmod + 1152 MAC, Poseidon2 736 mulmod.
+# These two are bound by multiplies, so their op rate is set against the
+# measured IMAD issue rate.  Keccak (64-bit logic on the ALU pipe, where one
+# LOP3 does a three-input XOR) and Monolith (byte-wise Bars on the ALU pipe,
+# concrete layers on the FP64 pipe) are not: an op count set against the IMAD
+# rate reads above 1 for them, so the sweep names their bound instead.
+OPS_PER_PERM = {0: 15378, 3: 7360}
+OTHER_BOUND = {1: "ALU pipe (logic of keccak-f on 32-bit halves; 99 % in ncu)",
+               4: "issue (ALU Bars + FP64 concrete layers; 78 % issue in ncu)",
+               2: "IMAD pipe (254-bit Montgomery products)"}
 
 # DRAM bytes (read + write) per step of each roofline's kernels, from one ncu
 # capture of this bench's default workload (profiles/ holds the commands and
@@ -390,15 +396,17 @@ def main() -> None:
         peaks = measured_peaks()
         hbm_peak = peaks.get("hbm_gbs")
         int_peak = int32_peak()
-        ops = PERMS * OPS_PER_PERM[HASH]
+        counted = HASH in OPS_PER_PERM  # multiply-bound hashers; the others carry their bound by name
+        ops = PERMS * OPS_PER_PERM.get(HASH, 0)
         roof = {
             "kernel": f"Merkle build (leaf sponge + levels + cap), {HASH_NAME}",
-            "bound": "int32", "unit": "Gop/s",
-            "achieved": ops / (t_mk * 1e-3) / 1e9,
+            "bound": "int32" if counted else OTHER_BOUND[HASH], "unit": "Gop/s",
+            "achieved": ops / (t_mk * 1e-3) / 1e9 if counted else None,
             "peak": int_peak / 1e9 if int_peak else None,
-            "frac": (ops / (t_mk * 1e-3)) / int_peak if int_peak else None,
+            "frac": (ops / (t_mk * 1e-3)) / int_peak if int_peak and counted else None,
             "traffic": NCU_TRAFFIC.get(("merkle", HASH, B, LG)),
-            "work_per_launch": f"{PERMS} {HASH_NAME} permutations x {OPS_PER_PERM[HASH]} INT32 multiply-class ops",
+            "work_per_launch": (f"{PERMS} {HASH_NAME} permutations x {OPS_PER_PERM[HASH]} INT32 multiply-class ops"
+                                if counted else f"{PERMS} {HASH_NAME} permutations"),
             "peak_source": "INT32 IMAD issue rate measured live by zeknox_b200/libzkprobe.so (MEASURED_PEAKS.json "
                            "has no integer figure)",
             "ms_per_launch": t_mk,
@@ -546,6 +554,8 @@ def run_sweep(args):
         ops = perms * OPS_PER_PERM.get(ht, 0)
         res[name] = {"ms": ms, "perm_per_s": perms / (ms * 1e-3), "leaf_elems_per_s": nl * w / (ms * 1e-3),
                      "int32_frac": ops / (ms * 1e-3) / peak if peak and ht in OPS_PER_PERM else None}
+        if ht in OTHER_BOUND:
+            res[name]["bound"] = OTHER_BOUND[ht]
     if args.no_cpu_baseline:
         print(json.dumps(res), flush=True)
         return
