@@ -1,7 +1,8 @@
 // Device hashers of the Merkle path: Poseidon, Poseidon2, Monolith
 // (Goldilocks, width 12), Poseidon-BN128 and Keccak-256 over Goldilocks words,
 // each one thread per hash with the whole state in registers; Poseidon also
-// on six and on two threads per hash (end of file) for latency-bound work.
+// on six and on two threads per hash, Poseidon2 also on six (end of file), for
+// latency-bound work.
 //
 // Semantics follow zeknox:
 //   Poseidon   native/poseidon/poseidon.cu:602-791 (4 full, 22 partial,
