@@ -114,27 +114,36 @@ def field_elems(seed: int, count: int) -> np.ndarray:
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons, sampled during the timed region."""
+    """nvidia-smi clocks / throttle reasons, sampled during the timed region.
 
-    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    nvidia-smi samples every 20 ms from a moment before the region starts (its
+    start-up and NVML initialisation take up to a few hundred ms), and only the
+    samples whose timestamps fall inside the region are summarised."""
+
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    LEAD_S = 0.4  # sampler running before the region starts
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.out = ""
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(self.LEAD_S)
         except OSError:
             self.proc = None
+        self.t0 = time.time()
         return self
 
     def __exit__(self, *exc):
-        self.out = ""
+        self.t1 = time.time()
         if self.proc:
             self.proc.terminate()
             try:
@@ -143,23 +152,33 @@ class ClockSampler:
                 self.proc.kill()
                 self.out, _ = self.proc.communicate()
 
+    @staticmethod
+    def _stamp(text: str) -> float | None:
+        import datetime
+
+        try:
+            return datetime.datetime.strptime(text, "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
+
     def summary(self) -> dict:
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for ln in (self.out or "").splitlines():
             f = [x.strip() for x in ln.split(",")]
-            if len(f) < 8:
+            if len(f) < 9:
                 continue
             try:
-                sm.append(float(f[0]))
-                mx = float(f[1])
+                rows.append((self._stamp(f[0]), float(f[1]), float(f[2]), f[5:9]))
             except ValueError:
                 continue
-            for name, v in zip(names, f[4:8]):
-                if v.lower() == "active":
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        inside = [r for r in rows if r[0] is not None and self.t0 is not None and self.t0 <= r[0] <= self.t1]
+        use = inside or rows  # no usable timestamps: every sample, flagged below
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = {n for r in use for n, v in zip(names, r[3]) if v.lower() == "active"}
+        sm = [r[1] for r in use]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": use[-1][2] if use else None,
+                "reasons": sorted(reasons), "samples": len(sm), "interval_ms": 20,
+                "window": "timed region" if inside else "whole sampler run"}
 
 
 def measured_peaks() -> dict:
