@@ -2,6 +2,7 @@
 from zeknox's sources) at full benchmark sizes, on the same B200 and the same
 device buffers:
 
+* compute_batched_ntt forward and inverse on 135 x 2^15 and 135 x 2^18;
 * the default commit (135 x 2^15 coefficients, rate 3, Poseidon, cap 4)
   through the drop-in ABI: compute_batched_lde -> compute_transpose_rev ->
   fill_digests_buf_linear_gpu_with_gpu_ptr, every output compared word for
@@ -55,6 +56,8 @@ def ref():
     L.init_twiddle_factors.restype = RustError
     L.init_coset.argtypes = [sz, sz, u64]
     L.init_coset.restype = RustError
+    L.compute_batched_ntt.argtypes = [sz, vp, u32, ctypes.c_int, NTTConfig]
+    L.compute_batched_ntt.restype = RustError
     L.compute_batched_lde.argtypes = [sz, vp, vp, u32, ctypes.c_int, NTTConfig]
     L.compute_batched_lde.restype = RustError
     L.compute_transpose_rev.argtypes = [sz, vp, vp, u32, TransposeConfig]
@@ -126,6 +129,35 @@ def test_default_commit_equals_and_outruns_the_reference_build(zk, ref, oracle):
              "speedup": {k: times["reference"][k] / times["ours"][k] for k in times["ours"]}}
     _record(entry)
     assert times["ours"]["total_ms"] <= times["reference"]["total_ms"], entry
+
+
+@pytest.mark.parametrize("lg", [15, 18])
+@pytest.mark.parametrize("direction", [0, 1])
+def test_batched_ntt_equals_and_outruns_the_reference_build(zk, ref, oracle, lg, direction):
+    """compute_batched_ntt, in place on device buffers, 135 polynomials: 2^15
+    points is the iNTT of a values-input commit, 2^18 the LDE's domain."""
+    import torch
+
+    b = 135
+    x = torch.from_numpy(oracle.field_elems(0x5EED0003 + lg + direction, b << lg)).cuda()
+    cfg = zk.NTTConfig.default()
+    cfg.batches, cfg.are_inputs_on_device, cfg.are_outputs_on_device = b, True, True
+    assert ref.init_twiddle_factors(0, lg).code == 0
+    res = {}
+    for name, lib in (("reference", ref), ("ours", zk.capi.LIB)):
+        once = x.clone()
+        assert lib.compute_batched_ntt(0, once.data_ptr(), lg, direction, cfg).code == 0, name
+        work = x.clone()
+        t = _timed(lambda: lib.compute_batched_ntt(0, work.data_ptr(), lg, direction, cfg).code == 0 or
+                   pytest.fail(f"{name} NTT failed"))
+        torch.cuda.synchronize()
+        res[name] = (t, once)
+    assert torch.equal(res["ours"][1].view(torch.int64), res["reference"][1].view(torch.int64))
+    entry = {"case": f"{'inverse' if direction else 'forward'} NTT 135 x 2^{lg} (compute_batched_ntt, device)",
+             "reference_ms": res["reference"][0], "ours_ms": res["ours"][0],
+             "speedup": res["reference"][0] / res["ours"][0]}
+    _record(entry)
+    assert res["ours"][0] <= res["reference"][0], entry
 
 
 @pytest.mark.parametrize("ht,lg_leaves", [(0, 20), (3, 20), (1, 20), (4, 20), (2, 16), (0, 13), (3, 13), (1, 13), (4, 13)])
