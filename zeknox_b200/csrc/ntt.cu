@@ -35,6 +35,129 @@ namespace {
 constexpr int kNttThreads = 256;
 constexpr int kLinesElems = 1 << 13;  // elements per group held in shared memory
 
+// Field operations of the transform passes.  The passes are bound by the ALU
+// pipe (64-bit adds, subtracts, selects and reduction carries on 32-bit
+// halves), while the FMA pipe, which runs the multiply-adds, has room.  So
+// these forms take no select and move the folds by 2^64 = 2^32 - 1 (mod p)
+// onto multiply-adds: x + k (2^32 - 1) for k in {0, 1} is one mad.wide.u32,
+// and r + h (2^32 - 1) with its carry-out is a mad.lo.cc / madc.hi.cc pair.
+// Results equal gl_add, gl_sub and gl_mul (canonical in, canonical out).
+constexpr uint32_t kLo32 = 0xffffffffu;  // 2^32 - 1 = 2^64 mod p
+
+__device__ __forceinline__ uint64_t fold_k(uint32_t k, uint64_t x) {  // x + k (2^32 - 1) mod 2^64
+    uint64_t r;
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(r) : "r"(k), "r"(kLo32), "l"(x));
+    return r;
+}
+
+// Canonical form of any u64: x >= p exactly when x + (2^32 - 1) carries, and
+// then x - p = x + (2^32 - 1) mod 2^64.
+__device__ __forceinline__ uint64_t nt_canon(uint64_t x) {
+    uint32_t k;
+    asm("{\n\t"
+        ".reg .u32 t;\n\t"
+        "add.cc.u32 t, %1, %3;\n\t"
+        "addc.cc.u32 t, %2, 0;\n\t"
+        "addc.u32 %0, 0, 0;\n\t"
+        "}"
+        : "=r"(k)
+        : "r"((uint32_t)x), "r"((uint32_t)(x >> 32)), "r"(kLo32));
+    return fold_k(k, x);
+}
+
+// a - b mod p for canonical a, b.  On a borrow, d + p = d - (2^32 - 1) mod
+// 2^64: the low word minus 0xffffffff (that is, plus one), and a borrow from
+// the high word exactly when that does not wrap.
+__device__ __forceinline__ uint64_t nt_sub(uint64_t a, uint64_t b) {
+    uint32_t lo, hi;
+    asm("{\n\t"
+        ".reg .u32 bw;\n\t"
+        "sub.cc.u32 %0, %2, %4;\n\t"
+        "subc.cc.u32 %1, %3, %5;\n\t"
+        "subc.u32 bw, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, bw;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        "}"
+        : "=r"(lo), "=r"(hi)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    return ((uint64_t)hi << 32) | lo;
+}
+
+// a + b mod p for canonical a, b: s = a + b mod 2^64 takes + (2^32 - 1) when the
+// sum carried out of 2^64 or s >= p (at most one of the two happens).
+__device__ __forceinline__ uint64_t nt_add(uint64_t a, uint64_t b) {
+    uint32_t s0, s1, m;
+    asm("{\n\t"
+        ".reg .u32 c0, t;\n\t"
+        "add.cc.u32 %0, %3, %5;\n\t"
+        "addc.cc.u32 %1, %4, %6;\n\t"
+        "addc.u32 c0, 0, 0;\n\t"
+        "add.cc.u32 t, %0, %7;\n\t"
+        "addc.cc.u32 t, %1, 0;\n\t"
+        "addc.u32 %2, c0, 0;\n\t"
+        "}"
+        : "=r"(s0), "=r"(s1), "=r"(m)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)), "r"(kLo32));
+    return fold_k(m, ((uint64_t)s1 << 32) | s0);
+}
+
+// (h1, h0, l1, l0) 128-bit -> u64 congruent mod p (not canonical):
+// l - h1 (minus 2^32 - 1 on a borrow, as in nt_sub), then + h0 (2^32 - 1)
+// with its carry folded once more (it cannot carry again).
+__device__ __forceinline__ uint64_t nt_reduce128(uint32_t l0, uint32_t l1, uint32_t h0, uint32_t h1) {
+    uint32_t r0, r1, k;
+    asm("{\n\t"
+        ".reg .u32 b;\n\t"
+        "sub.cc.u32 %0, %3, %6;\n\t"
+        "subc.cc.u32 %1, %4, 0;\n\t"
+        "subc.u32 b, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, b;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        "mad.lo.cc.u32 %0, %5, %7, %0;\n\t"
+        "madc.hi.cc.u32 %1, %5, %7, %1;\n\t"
+        "addc.u32 %2, 0, 0;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1), "=r"(k)
+        : "r"(l0), "r"(l1), "r"(h0), "r"(h1), "r"(kLo32));
+    return fold_k(k, ((uint64_t)r1 << 32) | r0);
+}
+
+__device__ __forceinline__ uint64_t nt_mul(uint64_t a, uint64_t b) {
+    uint64_t lo, hi;
+    mul_wide(a, b, lo, hi);
+    return nt_canon(nt_reduce128((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32)));
+}
+
+// Multiplication by the 8th roots of unity.  In this field 2^96 = -1, so 2 has
+// order 192 and the 8th roots are powers of 2: for omega_8 = 7^((p-1)/8)
+// (the root every table here is built from), omega_8 = 2^120 = -2^24,
+// omega_8^2 = omega_4 = 2^48, omega_8^3 = -2^72, and the inverses are 2^72,
+// -2^48, 2^24.  None of the three is a 64 x 64 product: x * 2^24 and x * 2^48
+// are a shift and one reduction, x * 2^72 is two shifts and a subtraction.
+__device__ __forceinline__ uint64_t gl_mul2_24(uint64_t x) {
+    // x 2^24 = lo + h 2^64 with h < 2^24: lo + h (2^32 - 1), its carry folded.
+    uint32_t r0 = (uint32_t)(x << 24), r1 = (uint32_t)(x >> 8), k;
+    asm("{\n\t"
+        "mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
+        "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
+        "addc.u32 %2, 0, 0;\n\t"
+        "}"
+        : "+r"(r0), "+r"(r1), "=r"(k)
+        : "r"((uint32_t)(x >> 40)), "r"(kLo32));
+    return nt_canon(fold_k(k, ((uint64_t)r1 << 32) | r0));
+}
+__device__ __forceinline__ uint64_t gl_mul2_48(uint64_t x) {
+    const uint64_t lo = x << 48, hi = x >> 16;
+    return nt_canon(nt_reduce128((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32)));
+}
+// x * 2^72 for canonical x: with x = xh 2^24 + xl (xl < 2^24), 2^96 = -1 gives
+// x 2^72 = xl 2^72 - xh = xl (2^40 - 2^8) - xh (mod p), where both
+// xl (2^40 - 2^8) and xh are below p.
+__device__ __forceinline__ uint64_t gl_mul2_72(uint64_t x) {
+    const uint64_t xl = x & 0xffffffull, xh = x >> 24;
+    return nt_sub((xl << 40) - (xl << 8), xh);
+}
+
 struct PassArgs {
     const uint64_t *src;
     uint64_t *dst;
@@ -71,7 +194,7 @@ struct PassArgs {
 };
 
 __device__ __forceinline__ uint64_t pow2l(const uint64_t *lo, const uint64_t *hi, uint32_t h, uint64_t e) {
-    return gl_mul(__ldg(lo + (e & ((1ull << h) - 1))), __ldg(hi + (e >> h)));
+    return nt_mul(__ldg(lo + (e & ((1ull << h) - 1))), __ldg(hi + (e >> h)));
 }
 // b^e from the one-load table when there is one, else from the two-level table.
 __device__ __forceinline__ uint64_t pow_at(const uint64_t *full, const uint64_t *lo, const uint64_t *hi, uint32_t h,
@@ -85,8 +208,8 @@ __device__ __forceinline__ uint32_t brev_bits(uint32_t x, uint32_t bits) {
 
 // DIF butterfly with w = 1: (u, v) -> (u + v, u - v).
 __device__ __forceinline__ void bfly1(uint64_t &u, uint64_t &v) {
-    const uint64_t d = gl_sub(u, v);
-    u = gl_add(u, v);
+    const uint64_t d = nt_sub(u, v);
+    u = nt_add(u, v);
     v = d;
 }
 
@@ -98,53 +221,36 @@ __device__ __forceinline__ void cp_async8(uint64_t *smem_dst, const uint64_t *gm
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Multiplication by the 8th roots of unity.  In this field 2^96 = -1, so 2 has
-// order 192 and the 8th roots are powers of 2: for omega_8 = 7^((p-1)/8)
-// (the root every table here is built from), omega_8 = 2^120 = -2^24,
-// omega_8^2 = omega_4 = 2^48, omega_8^3 = -2^72, and the inverses are 2^72,
-// -2^48, 2^24.  None of the three is a 64 x 64 product: x * 2^24 and x * 2^48
-// are a shift and one reduction, x * 2^72 is two shifts and a subtraction.
-__device__ __forceinline__ uint64_t gl_mul2_24(uint64_t x) { return gl_reduce96(x << 24, (uint32_t)(x >> 40)); }
-__device__ __forceinline__ uint64_t gl_mul2_48(uint64_t x) { return gl_reduce128(x << 48, x >> 16); }
-// x * 2^72 for canonical x: with x = xh 2^24 + xl (xl < 2^24), 2^96 = -1 gives
-// x 2^72 = xl 2^72 - xh = xl (2^40 - 2^8) - xh (mod p), where
-// xl (2^40 - 2^8) < p and xh < 2^40; one correction on borrow keeps it canonical.
-__device__ __forceinline__ uint64_t gl_mul2_72(uint64_t x) {
-    const uint64_t xl = x & 0xffffffull, xh = x >> 24;
-    const uint64_t a = (xl << 40) - (xl << 8);
-    return a >= xh ? a - xh : a - xh - ZK_EPS;  // on borrow, 2^64 - eps = p is added back
-}
-
 // 8-point DFT in place (DIF radix-2 inside, natural order in, bit-reversed
 // out), with the direction's 8th roots.  Negated roots swap the operands of
 // the subtraction instead of negating.
 __device__ __forceinline__ void dft8(uint64_t x[8], bool inv) {
     uint64_t d[4];
-    d[0] = gl_sub(x[0], x[4]);
+    d[0] = nt_sub(x[0], x[4]);
     if (!inv) {
-        d[1] = gl_mul2_24(gl_sub(x[5], x[1]));      // (x1 - x5) * (-2^24)
-        d[2] = gl_mul2_48(gl_sub(x[2], x[6]));      // (x2 - x6) * 2^48
-        d[3] = gl_mul2_72(gl_sub(x[7], x[3]));      // (x3 - x7) * (-2^72)
+        d[1] = gl_mul2_24(nt_sub(x[5], x[1]));      // (x1 - x5) * (-2^24)
+        d[2] = gl_mul2_48(nt_sub(x[2], x[6]));      // (x2 - x6) * 2^48
+        d[3] = gl_mul2_72(nt_sub(x[7], x[3]));      // (x3 - x7) * (-2^72)
     } else {
-        d[1] = gl_mul2_72(gl_sub(x[1], x[5]));      // * 2^72
-        d[2] = gl_mul2_48(gl_sub(x[6], x[2]));      // * (-2^48)
-        d[3] = gl_mul2_24(gl_sub(x[3], x[7]));      // * 2^24
+        d[1] = gl_mul2_72(nt_sub(x[1], x[5]));      // * 2^72
+        d[2] = gl_mul2_48(nt_sub(x[6], x[2]));      // * (-2^48)
+        d[3] = gl_mul2_24(nt_sub(x[3], x[7]));      // * 2^24
     }
 #pragma unroll
-    for (int k = 0; k < 4; k++) x[k] = gl_add(x[k], x[k + 4]);
+    for (int k = 0; k < 4; k++) x[k] = nt_add(x[k], x[k + 4]);
 #pragma unroll
     for (int k = 0; k < 4; k++) x[k + 4] = d[k];
     // span 2: (0,2), (1,3)*omega_4, (4,6), (5,7)*omega_4
 #pragma unroll
     for (int h = 0; h < 8; h += 4) {
-        const uint64_t a0 = gl_add(x[h], x[h + 2]), a2 = gl_sub(x[h], x[h + 2]);
-        const uint64_t a1 = gl_add(x[h + 1], x[h + 3]);
-        const uint64_t a3 = inv ? gl_mul2_48(gl_sub(x[h + 3], x[h + 1])) : gl_mul2_48(gl_sub(x[h + 1], x[h + 3]));
+        const uint64_t a0 = nt_add(x[h], x[h + 2]), a2 = nt_sub(x[h], x[h + 2]);
+        const uint64_t a1 = nt_add(x[h + 1], x[h + 3]);
+        const uint64_t a3 = inv ? gl_mul2_48(nt_sub(x[h + 3], x[h + 1])) : gl_mul2_48(nt_sub(x[h + 1], x[h + 3]));
         // span 1
-        x[h] = gl_add(a0, a1);
-        x[h + 1] = gl_sub(a0, a1);
-        x[h + 2] = gl_add(a2, a3);
-        x[h + 3] = gl_sub(a2, a3);
+        x[h] = nt_add(a0, a1);
+        x[h + 1] = nt_sub(a0, a1);
+        x[h + 2] = nt_add(a2, a3);
+        x[h + 3] = nt_sub(a2, a3);
     }
 }
 
@@ -177,7 +283,7 @@ __device__ __forceinline__ void smem_dif(uint64_t *sm, const uint64_t *tw, uint3
             if (o != 0) {
                 constexpr uint32_t rev3[8] = {0, 4, 2, 6, 1, 5, 3, 7};
 #pragma unroll
-                for (int j = 1; j < 8; j++) x[j] = gl_mul(x[j], tw[(o * rev3[j]) << sh8]);
+                for (int j = 1; j < 8; j++) x[j] = nt_mul(x[j], tw[(o * rev3[j]) << sh8]);
             }
 #pragma unroll
             for (int k = 0; k < 8; k++) sm[(e0 + k * q) * tp + t] = x[k];
@@ -191,12 +297,12 @@ __device__ __forceinline__ void smem_dif(uint64_t *sm, const uint64_t *tw, uint3
             const uint32_t t = u & (T - 1), e0 = (u >> lg_t) << 2;
             const uint64_t x0 = sm[e0 * tp + t], x1 = sm[(e0 + 1) * tp + t], x2 = sm[(e0 + 2) * tp + t],
                            x3 = sm[(e0 + 3) * tp + t];
-            const uint64_t a0 = gl_add(x0, x2), a2 = gl_sub(x0, x2), a1 = gl_add(x1, x3);
-            const uint64_t a3 = inv ? gl_mul2_48(gl_sub(x3, x1)) : gl_mul2_48(gl_sub(x1, x3));
-            sm[e0 * tp + t] = gl_add(a0, a1);
-            sm[(e0 + 1) * tp + t] = gl_sub(a0, a1);
-            sm[(e0 + 2) * tp + t] = gl_add(a2, a3);
-            sm[(e0 + 3) * tp + t] = gl_sub(a2, a3);
+            const uint64_t a0 = nt_add(x0, x2), a2 = nt_sub(x0, x2), a1 = nt_add(x1, x3);
+            const uint64_t a3 = inv ? gl_mul2_48(nt_sub(x3, x1)) : gl_mul2_48(nt_sub(x1, x3));
+            sm[e0 * tp + t] = nt_add(a0, a1);
+            sm[(e0 + 1) * tp + t] = nt_sub(a0, a1);
+            sm[(e0 + 2) * tp + t] = nt_add(a2, a3);
+            sm[(e0 + 3) * tp + t] = nt_sub(a2, a3);
         }
         __syncthreads();
     } else if (s == 0) {  // span 1
@@ -267,17 +373,17 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
             uint64_t v = 0;
             if (i < a.n_valid) {
                 if (rr >= 2) {
-                    v = gl_canon(sm[((1u << lv) + e) * tp + t]);
-                    if (a.pre_full) v = gl_mul(v, sm[((2u << lv) + e) * tp + t]);
-                    else if (a.pre_lo) v = gl_mul(v, pow2l(a.pre_lo, a.pre_hi, a.pre_h, i));
+                    v = nt_canon(sm[((1u << lv) + e) * tp + t]);
+                    if (a.pre_full) v = nt_mul(v, sm[((2u << lv) + e) * tp + t]);
+                    else if (a.pre_lo) v = nt_mul(v, pow2l(a.pre_lo, a.pre_hi, a.pre_h, i));
                 } else {
-                    v = gl_canon(src[i]);
-                    if (a.pre_lo) v = gl_mul(v, pow_at(a.pre_full, a.pre_lo, a.pre_hi, a.pre_h, i));
+                    v = nt_canon(src[i]);
+                    if (a.pre_lo) v = nt_mul(v, pow_at(a.pre_full, a.pre_lo, a.pre_hi, a.pre_h, i));
                 }
             }
             sm[e * tp + t] = v;
             for (uint32_t b = 1; b < (1u << rr); b++)
-                sm[((b << lv) + e) * tp + t] = gl_mul(v, tw[(e * brev_bits(b, rr)) & (L - 1)]);
+                sm[((b << lv) + e) * tp + t] = nt_mul(v, tw[(e * brev_bits(b, rr)) & (L - 1)]);
         }
         smem_dif(sm, tw, l, (int)lv - 1, a.lg_t, tp, a.inverse != 0);
         // store with the inter-pass twiddle w_N^((r0 + t) k Q): one table load
@@ -289,16 +395,16 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
         if (a.tw_full) {
             for (uint32_t k = k0; k < L; k += dk) {
                 const uint64_t tw_k = __ldg(a.tw_full + (((r * k) << a.lg_pre) & nmask));
-                dst[base + ((uint64_t)k << lg_s) + r] = gl_mul(sm[brev_bits(k, l) * tp + t], tw_k);
+                dst[base + ((uint64_t)k << lg_s) + r] = nt_mul(sm[brev_bits(k, l) * tp + t], tw_k);
             }
             return;
         }
         uint64_t twk = pow2l(a.tw_lo, a.tw_hi, a.tw_h, ((r * k0) << a.lg_pre) & nmask);
         const uint64_t step = pow2l(a.tw_lo, a.tw_hi, a.tw_h, ((r * dk) << a.lg_pre) & nmask);
         for (uint32_t k = k0; k < L; k += dk) {
-            const uint64_t v = gl_mul(sm[brev_bits(k, l) * tp + t], twk);
+            const uint64_t v = nt_mul(sm[brev_bits(k, l) * tp + t], twk);
             dst[base + ((uint64_t)k << lg_s) + r] = v;
-            twk = gl_mul(twk, step);
+            twk = nt_mul(twk, step);
         }
         return;
     }
@@ -329,8 +435,8 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
         if (t < nlines) {
             if (a.kind == 2) {
                 if (e < a.n_valid) {
-                    v = gl_canon(a.src[line_src(t) + e]);
-                    if (a.pre_lo) v = gl_mul(v, pow_at(a.pre_full, a.pre_lo, a.pre_hi, a.pre_h, e));
+                    v = nt_canon(a.src[line_src(t) + e]);
+                    if (a.pre_lo) v = nt_mul(v, pow_at(a.pre_full, a.pre_lo, a.pre_hi, a.pre_h, e));
                 }
             } else {
                 cp_async8(&sm[e * tp + t], a.src + line_src(t) + e);
@@ -348,8 +454,8 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
             const uint32_t t = idx & (T - 1), k = idx >> a.lg_t;
             uint64_t v = sm[brev_bits(k, l) * tp + t];
             const uint64_t o = c0 + t + ((uint64_t)k << a.lg_pre);
-            if (a.post_lo) v = gl_mul(v, pow_at(a.post_full, a.post_lo, a.post_hi, a.post_h, o));
-            if (a.scale != 1) v = gl_mul(v, a.scale);
+            if (a.post_lo) v = nt_mul(v, pow_at(a.post_full, a.post_lo, a.post_hi, a.post_h, o));
+            if (a.scale != 1) v = nt_mul(v, a.scale);
             dst[o] = v;
         }
     } else if (a.to_leaves) {
@@ -365,8 +471,8 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
             const uint32_t k = idx & (L - 1), t = idx >> l;
             if (t >= nlines) continue;
             uint64_t v = sm[brev_bits(k, l) * tp + t];
-            if (a.post_lo) v = gl_mul(v, pow_at(a.post_full, a.post_lo, a.post_hi, a.post_h, k));
-            if (a.scale != 1) v = gl_mul(v, a.scale);
+            if (a.post_lo) v = nt_mul(v, pow_at(a.post_full, a.post_lo, a.post_hi, a.post_h, k));
+            if (a.scale != 1) v = nt_mul(v, a.scale);
             a.dst[(poly0 + t) * a.dst_poly_stride + k] = v;
         }
     }
