@@ -50,7 +50,7 @@ OTHER_BOUND = {1: "ALU pipe (logic of keccak-f on 32-bit halves; 99 % in ncu)",
 # figures); None for workloads that were not captured.
 NCU_TRAFFIC = {
     ("merkle", 0, 135, 18): 331.5e6,      # merkle_leaves 317.9 MB + 4 wide levels 4.0 MB each + narrow levels
-    ("lde_leaves", 135, 18): 879.6e6,     # ntt_pass_kernel 258.4 MB + ntt_last_pass_leaves 621.2 MB
+    ("lde_leaves", 135, 18): 953.3e6,     # ntt_pass_kernel 261.6 MB + ntt_last_pass_leaves 691.7 MB
     ("transpose", 135, 18): 531.4e6,      # transpose_rev_kernel
 }
 
@@ -443,9 +443,9 @@ def main() -> None:
             "traffic": NCU_TRAFFIC.get(("lde_leaves", B, LG)), "algorithmic_bytes": hbm_bytes, "ms_per_launch": t_lde,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm_peak else None,
             # What does bound it, from ncu on this workload (column pass, leaves pass):
-            "compute_view": {"bound": "ALU pipe (64-bit modular arithmetic on 32-bit integer units)",
-                             "alu_pipe_pct": [71.2, 78.9], "issue_active_pct": [60.2, 69.7],
-                             "instructions_per_output_element": [232, 277],
+            "compute_view": {"bound": "integer issue (64-bit modular arithmetic on 32-bit units, ALU and FMA pipes)",
+                             "alu_pipe_pct": [57.3, 65.4], "fma_pipe_pct": [34.6, 36.9],
+                             "issue_active_pct": [63.4, 75.2], "instructions_per_output_element": [231, 269],
                              "source": "profiles/ntt_lde_to_leaves_135x2^15_rate3.md"},
         }
         roof_tr = {
