@@ -920,6 +920,8 @@ struct HexLanes {
     __device__ __forceinline__ bool real() const { return (threadIdx.x & 31) < 30; }
     __device__ __forceinline__ uint32_t group_in_warp() const { return base / 6; }
 };
+// Poseidon's group: its MDS rows in registers.  (The table argument gives the
+// Poseidon and Poseidon2 group forms one constructor signature.)
 struct HexGroup : HexLanes {
     double p2[6], q2[6];  // row t of A + B and A - B (with the diagonal term on row 0)
     double fix6;          // -2 d on thread 0 (lane 6 must not get the diagonal), else 0
