@@ -45,14 +45,42 @@ OTHER_BOUND = {1: "ALU pipe (logic of keccak-f on 32-bit halves; 99 % in ncu)",
                4: "issue (ALU Bars + FP64 concrete layers; 78 % issue in ncu)",
                2: "IMAD pipe (254-bit Montgomery products)"}
 
-# DRAM bytes (read + write) per step of each roofline's kernels, from one ncu
-# capture of this bench's default workload (profiles/ holds the commands and
-# figures); None for workloads that were not captured.
-NCU_TRAFFIC = {
-    ("merkle", 0, 135, 18): 331.5e6,      # merkle_leaves 317.9 MB + 4 wide levels 4.0 MB each + narrow levels
-    ("lde_leaves", 135, 18): 953.3e6,     # ntt_pass_kernel 261.6 MB + ntt_last_pass_leaves 691.7 MB
-    ("transpose", 135, 18): 531.4e6,      # transpose_rev_kernel
-}
+# Figures that come from an ncu capture (DRAM bytes per launch, thread
+# instructions per permutation) live in profiles/ncu_figures.json together with
+# the SHA-256 of the kernel sources they were captured from.  They are reported
+# only while the sources still hash to that value; after a kernel change they
+# read null until the capture is redone.
+PROFILE_FIGURES = ROOT / "profiles" / "ncu_figures.json"
+
+
+def kernel_sources_sha256() -> str:
+    import hashlib
+
+    h = hashlib.sha256()
+    for f in sorted((ROOT / "zeknox_b200" / "csrc").glob("*")):
+        if f.suffix in (".cu", ".cuh", ".h"):
+            h.update(f.name.encode())
+            h.update(f.read_bytes())
+    return h.hexdigest()
+
+
+def profile_figures() -> dict:
+    """{"source": ..., "kernels": {...}} from the capture of the current kernel sources, or {}."""
+    if not PROFILE_FIGURES.exists():
+        return {}
+    d = json.loads(PROFILE_FIGURES.read_text())
+    if d.get("sources_sha256") != kernel_sources_sha256():
+        return {}
+    return d
+
+
+def job_seed(config: int, j: int) -> int:
+    """Seed of job j of a multi-job configuration: (0x5EED0000 + config) xor SplitMix64's output for j."""
+    z = ((j + 1) * 0x9E3779B97F4A7C15) & (2**64 - 1)
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & (2**64 - 1)
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & (2**64 - 1)
+    z ^= z >> 31
+    return (0x5EED0000 + config) ^ z
 
 
 def max_over_ranks(values, dist, device) -> list:
@@ -260,11 +288,19 @@ def main() -> None:
     ap.add_argument("--hash", default="poseidon", choices=sorted(HASH_NAMES))
     ap.add_argument("--workload", default="commit", choices=["commit", "merkle", "sweep", "batched", "served", "fri"],
                     help="commit (default, the bench line); the others print their own JSON summary")
-    ap.add_argument("--jobs", type=int, default=0)
     ap.add_argument("--leaves", type=int, default=8192, help="leaf count of the merkle workload (a power of two)")
-    ap.add_argument("--streams", type=int, default=4)
+    ap.add_argument("--streams", type=int, default=4, help="internal streams of a batch / slots of the server")
     ap.add_argument("--budget-gb", type=int, default=120)
-    ap.add_argument("--rates", type=float, nargs="*", default=[0.25, 0.5, 0.75, 1.0, 1.25])
+    ap.add_argument("--sections", default="batched,served",
+                    help="multi-job sections added to the default (commit) line: batched (config 3), served (config 5)")
+    ap.add_argument("--batched-jobs", type=int, default=256)
+    ap.add_argument("--served-jobs", type=int, default=200, help="prefix of the seeded 10,000-job stream")
+    ap.add_argument("--served-rates", type=float, nargs="*", default=[0.75, 1.0],
+                    help="arrival rates as fractions of the plain path's measured capacity")
+    ap.add_argument("--served-repeats", type=int, default=1)
+    ap.add_argument("--served-replay", action="store_true",
+                    help="time the plain FIFO arm by a real-time replay at each rate")
+    ap.add_argument("--oracle-sample", type=int, default=6, help="jobs per section recomputed on the host")
     args = ap.parse_args()
     if args.workload != "commit" and args.impl == "ours":
         {"merkle": run_merkle_only, "sweep": run_sweep, "batched": run_batched, "served": run_served,
@@ -417,18 +453,38 @@ def main() -> None:
         int_peak = int32_peak()
         counted = HASH in OPS_PER_PERM  # multiply-bound hashers; the others carry their bound by name
         ops = PERMS * OPS_PER_PERM.get(HASH, 0)
+        prof = profile_figures()
+        pk = prof.get("kernels", {})
+        prof_src = (f"ncu capture of kernel sources sha256 {prof['sources_sha256'][:12]} "
+                    f"({prof.get('command', '')})") if prof else None
+        sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
+        sm_mhz = clk.summary().get("sm_mhz")
+        mk_key = f"merkle {HASH_NAME} {N}x{B} cap {CAP_H}"
+        lde_key = f"lde_leaves {B}x2^{LG_N} rate {RATE}"
+        tr_key = f"transpose_rev {B}x2^{LG}"
+        inst = pk.get(mk_key, {}).get("thread_inst_per_perm")
         roof = {
             "kernel": f"Merkle build (leaf sponge + levels + cap), {HASH_NAME}",
             "bound": "int32" if counted else OTHER_BOUND[HASH], "unit": "Gop/s",
             "achieved": ops / (t_mk * 1e-3) / 1e9 if counted else None,
             "peak": int_peak / 1e9 if int_peak else None,
             "frac": (ops / (t_mk * 1e-3)) / int_peak if int_peak and counted else None,
-            "traffic": NCU_TRAFFIC.get(("merkle", HASH, B, LG)),
+            "traffic": pk.get(mk_key, {}).get("dram_bytes_per_launch"),
             "work_per_launch": (f"{PERMS} {HASH_NAME} permutations x {OPS_PER_PERM[HASH]} INT32 multiply-class ops"
                                 if counted else f"{PERMS} {HASH_NAME} permutations"),
             "peak_source": "INT32 IMAD issue rate measured live by zeknox_b200/libzkprobe.so (MEASURED_PEAKS.json "
                            "has no integer figure)",
             "ms_per_launch": t_mk,
+            # What the kernel executes, against the SMs' issue rate (4 warp
+            # instructions per clock per SM): the op count above assumes the
+            # integer form of the MDS layer, which runs on the FP64 pipe here.
+            "issue_view": {
+                "thread_inst_per_perm": inst,
+                "achieved_warp_inst_per_s": inst * PERMS / 32 / (t_mk * 1e-3) if inst else None,
+                "peak_warp_inst_per_s": sm_count * 4 * sm_mhz * 1e6 if sm_mhz else None,
+                "frac": (inst * PERMS / 32 / (t_mk * 1e-3)) / (sm_count * 4 * sm_mhz * 1e6) if inst and sm_mhz else None,
+                "source": prof_src or "no ncu capture of the current kernel sources",
+                "peak_source": f"{sm_count} SMs x 4 issue slots x median SM clock sampled in the timed region"},
             # The same kernel against HBM: it reads the leaf matrix once and writes the digests.
             "hbm_view": {"algorithmic_bytes": B * N * 8 + (nd + nc) * 32,
                          "achieved_gbs": (B * N * 8 + (nd + nc) * 32) / (t_mk * 1e-3) / 1e9,
@@ -437,22 +493,20 @@ def main() -> None:
         }
         hbm_bytes = LDE_BYTES
         roof_hbm = {
-            "kernel": "LDE written as leaves (2 shared-memory NTT passes)", "bound": "hbm", "unit": "GB/s",
+            "kernel": "LDE written as leaves (shared-memory NTT passes)", "bound": "hbm", "unit": "GB/s",
             "achieved": hbm_bytes / (t_lde * 1e-3) / 1e9, "peak": hbm_peak,
             "frac": (hbm_bytes / (t_lde * 1e-3) / 1e9) / hbm_peak if hbm_peak else None,
-            "traffic": NCU_TRAFFIC.get(("lde_leaves", B, LG)), "algorithmic_bytes": hbm_bytes, "ms_per_launch": t_lde,
+            "traffic": pk.get(lde_key, {}).get("dram_bytes_per_launch"), "algorithmic_bytes": hbm_bytes,
+            "ms_per_launch": t_lde,
+            "thread_inst_per_output_elem": pk.get(lde_key, {}).get("thread_inst_per_elem"),
+            "figures_source": prof_src if lde_key in pk else "no ncu capture of the current kernel sources",
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm_peak else None,
-            # What does bound it, from ncu on this workload (column pass, leaves pass):
-            "compute_view": {"bound": "integer issue (64-bit modular arithmetic on 32-bit units, ALU and FMA pipes)",
-                             "alu_pipe_pct": [57.3, 65.4], "fma_pipe_pct": [34.6, 36.9],
-                             "issue_active_pct": [63.4, 75.2], "instructions_per_output_element": [231, 269],
-                             "source": "profiles/ntt_lde_to_leaves_135x2^15_rate3.md"},
         }
         roof_tr = {
             "kernel": "compute_transpose_rev (bit-reversing column -> leaf transpose, plain path)", "bound": "hbm",
             "unit": "GB/s", "achieved": TRANSPOSE_BYTES / (p_tr * 1e-3) / 1e9, "peak": hbm_peak,
             "frac": (TRANSPOSE_BYTES / (p_tr * 1e-3) / 1e9) / hbm_peak if hbm_peak else None,
-            "traffic": NCU_TRAFFIC.get(("transpose", B, LG)), "algorithmic_bytes": TRANSPOSE_BYTES,
+            "traffic": pk.get(tr_key, {}).get("dram_bytes_per_launch"), "algorithmic_bytes": TRANSPOSE_BYTES,
             "ms_per_launch": p_tr,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm_peak else None,
         }
@@ -497,6 +551,15 @@ def main() -> None:
                                           else "the oracle port"),
             }
             out["check"]["cap_equals_cpu_reference"] = bool(np.array_equal(cpu_cap.reshape(-1, 4), cap_e2e))
+        if world == 1:
+            # the metric's "batched vs plain" and "p99 latency": configs 3 and 5 in the same line
+            secs = [x for x in args.sections.split(",") if x]
+            del lde_out, leaves, digests, cap, coeffs
+            torch.cuda.empty_cache()
+            if "batched" in secs:
+                out["batched"] = batched_section(args, zk, torch, not args.no_cpu_baseline)
+            if "served" in secs:
+                out["served"] = served_section(args, zk, torch, not args.no_cpu_baseline)
         print(json.dumps(out), flush=True)
     if dist is not None:
         dist.barrier()
@@ -504,10 +567,9 @@ def main() -> None:
 
 
 # ------------------------------------------------------------------ other workloads
-def _device_pool(torch, elems: int, seed: int):
-    """Device buffer of canonical field elements (values < 2^62), shared by jobs as input."""
-    g = torch.Generator(device="cuda").manual_seed(seed)
-    return torch.randint(0, 2**62, (elems,), generator=g, device="cuda", dtype=torch.int64).view(torch.uint64)
+def _field_tensor(zk, torch, elems: int, seed: int):
+    """Device tensor of field elements uniform in [0, p): fill_field(seed)."""
+    return zk.fill_field(torch.empty(elems, dtype=torch.uint64, device="cuda"), seed)
 
 
 def _ev_ms(torch, fn, reps=1):
@@ -560,7 +622,7 @@ def run_sweep(args):
     import zeknox_b200 as zk
 
     nl, w, ch = 1 << 20, 135, 4
-    leaves = _device_pool(torch, nl * w, 0x5EED0004).view(nl, w)
+    leaves = _field_tensor(zk, torch, nl * w, 0x5EED0004).view(nl, w)
     peak = int32_peak()
     res = {"workload": "merkle sweep 2^20 x 135, cap_height 4", "int32_peak_gops": peak / 1e9 if peak else None}
     for name, ht in (("poseidon", 0), ("poseidon2", 3), ("keccak", 1), ("monolith", 4), ("poseidonbn128", 2)):
@@ -603,7 +665,7 @@ def run_fri(args):
 
     lg_n, rate, arities, ch = 15, 3, [4, 4, 4], 4
     n = 1 << lg_n
-    coeffs = _device_pool(torch, 2 * n, 0x5EED0006).view(2, n)
+    coeffs = _field_tensor(zk, torch, 2 * n, 0x5EED0006).view(2, n)
     P = zk.P
 
     def challenge(i, cap):
@@ -659,206 +721,395 @@ def run_fri(args):
 
 
 def _jobs(seed, count, lg_lo, lg_hi, b_lo, b_hi, rates):
+    """The seeded job list of a multi-job configuration: (lg_n, polynomials, rate_bits) per job."""
     rng = np.random.default_rng(seed)
     return [(int(rng.integers(lg_lo, lg_hi + 1)), int(rng.integers(b_lo, b_hi + 1)), int(rng.choice(rates)))
             for _ in range(count)]
 
 
-def _plain_job(zk, torch, coeffs, lg_n, rate, b, ch, bufs):
-    """One job through zeknox's drop-in C ABI: LDE matrix, transpose, forest, sync."""
-    N = 1 << (lg_n + rate)
-    lde_out, leaves, digests, cap = bufs
-    cfg = zk.NTTConfig.default()
-    cfg.batches, cfg.extension_rate_bits, cfg.with_coset = b, rate, True
-    cfg.are_inputs_on_device = cfg.are_outputs_on_device = True
-    zk.lde_batch(0, lde_out.data_ptr(), coeffs.data_ptr(), lg_n, cfg)
-    t = zk.TransposeConfig.default()
-    t.batches, t.are_inputs_on_device, t.are_outputs_on_device = b, True, True
-    zk.transpose_rev_batch(0, leaves.data_ptr(), lde_out.data_ptr(), lg_n + rate, t)
-    zk.fill_digests_buf_linear_gpu_with_gpu_ptr(digests.data_ptr(), cap.data_ptr(), leaves.data_ptr(),
-                                                2 * (N - (1 << ch)), 1 << ch, N, b, ch, 0, 0)
-    torch.cuda.synchronize()
+def fifo_latencies(arrivals, service):
+    """One server, first in first out: job j starts at max(its arrival, the end of
+    job j - 1) and takes service[j].  -> (latency of each job, first arrival to last end)."""
+    end, lat = 0.0, []
+    for a, sv in zip(arrivals, service):
+        end = max(a, end) + sv
+        lat.append(end - a)
+    return lat, (end - arrivals[0]) if len(lat) else 0.0
 
 
-def run_batched(args):
-    """256 jobs: lg_n in 12..20, polys 4..200, rate 1..3, cap height 4, Poseidon; one zk_commit_batch
-    call per memory wave vs the plain per-job drop-in path."""
-    import torch
+def _pct(x, q):
+    return float(np.percentile(np.asarray(x, dtype=np.float64), q)) if len(x) else None
 
-    import zeknox_b200 as zk
 
-    jobs = _jobs(0x5EED0003, args.jobs or 256, 12, 20, 4, 200, [1, 2, 3])
+class DropIn:
+    """One job at a time through a library's zeknox C ABI (this library's, or
+    zeknox's own build): compute_batched_lde -> compute_transpose_rev ->
+    fill_digests_buf_linear_gpu_with_gpu_ptr on device buffers, then the cap.
+
+    A job whose LDE matrix does not fit the LDE buffer (its footprint, LDE
+    matrix plus leaves, exceeds HBM) streams: the LDE and transpose run on
+    slices of polynomials, each transposed slice copied into its columns of
+    the leaf matrix (cudaMemcpy2DAsync), then the tree of the whole matrix."""
+
+    def __init__(self, torch, lib, check, max_in, max_leaves, max_n, lde_cap, cap_height=4):
+        self.torch, self.lib, self.check = torch, lib, check
+        self.lde = torch.empty(min(max_leaves, lde_cap), dtype=torch.uint64, device="cuda")
+        self.leaves = torch.empty(max_leaves, dtype=torch.uint64, device="cuda")
+        self.digests = torch.empty(8 * max_n, dtype=torch.uint64, device="cuda")
+        self.cap = torch.empty(4 << cap_height, dtype=torch.uint64, device="cuda")
+        self.streamed = 0
+
+    def run(self, coeffs_ptr, lg_n, rate, b, ch, ht=0):
+        from zeknox_b200.capi import NTTConfig, TransposeConfig
+
+        torch, L = self.torch, self.lib
+        lg = lg_n + rate
+        N, n = 1 << lg, 1 << lg_n
+        cfg = NTTConfig.default()
+        cfg.extension_rate_bits, cfg.with_coset = rate, True
+        cfg.are_inputs_on_device = cfg.are_outputs_on_device = True
+        t = TransposeConfig.default()
+        t.are_inputs_on_device = t.are_outputs_on_device = True
+        if b * N <= self.lde.numel():
+            cfg.batches, t.batches = b, b
+            self.check(L.compute_batched_lde(0, self.lde.data_ptr(), coeffs_ptr, lg_n, 0, cfg))
+            self.check(L.compute_transpose_rev(0, self.leaves.data_ptr(), self.lde.data_ptr(), lg, t))
+        else:
+            self.streamed += 1
+            g = self.lde.numel() // (2 * N)  # slice LDE and its transpose side by side in the LDE buffer
+            lde, tr = self.lde.data_ptr(), self.lde.data_ptr() + g * N * 8
+            for b0 in range(0, b, g):
+                nb = min(g, b - b0)
+                cfg.batches, t.batches = nb, nb
+                self.check(L.compute_batched_lde(0, lde, coeffs_ptr + b0 * n * 8, lg_n, 0, cfg))
+                self.check(L.compute_transpose_rev(0, tr, lde, lg, t))
+                # rows of nb words -> columns b0 .. b0 + nb of the b-word leaf rows (a strided device copy)
+                src = self.lde[g * N: g * N + nb * N].view(N, nb)
+                self.leaves[: b * N].view(N, b)[:, b0: b0 + nb].copy_(src)
+                torch.cuda.synchronize()
+        L.fill_digests_buf_linear_gpu_with_gpu_ptr(self.digests.data_ptr(), self.cap.data_ptr(),
+                                                   self.leaves.data_ptr(), 2 * (N - (1 << ch)), 1 << ch, N, b, ch,
+                                                   ht, 0)
+        cap = self.cap[: 4 << ch].cpu().numpy().copy()  # synchronises the legacy stream the tree ran on
+        return cap
+
+
+def _check_rust(r):
+    if r.code != 0:
+        raise RuntimeError(f"reference build: code {r.code}")
+
+
+def ref_gpu_build():
+    """zeknox's own sm_100a build (oracle/_ref/libzkref_gpu.so, compiled from its
+    sources) through its C ABI, for the baseline leg of the batched workload; None
+    when it was not built."""
+    import ctypes
+
+    so = ROOT / "oracle" / "_ref" / "libzkref_gpu.so"
+    if not so.exists():
+        return None
+    from zeknox_b200.capi import NTTConfig, RustError, TransposeConfig
+
+    L = ctypes.CDLL(str(so))
+    vp, sz, u32, u64 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64
+    for name, args in (("init_twiddle_factors", [sz, sz]), ("init_coset", [sz, sz, u64]),
+                       ("compute_batched_lde", [sz, vp, vp, u32, ctypes.c_int, NTTConfig]),
+                       ("compute_transpose_rev", [sz, vp, vp, u32, TransposeConfig])):
+        getattr(L, name).argtypes = args
+        getattr(L, name).restype = RustError
+    L.fill_digests_buf_linear_gpu_with_gpu_ptr.argtypes = [vp, vp, vp, u64, u64, u64, u64, u64, u64, u64]
+    L.fill_digests_buf_linear_gpu_with_gpu_ptr.restype = None
+    return L
+
+
+def _oracle_caps(sample, cap_height=4):
+    """Caps of (seed, lg_n, polys, rate) jobs computed on the host: the oracle's LDE and
+    transpose, zeknox's CPU Merkle path when built (else the oracle's)."""
+    from oracle import oracle as O
+
+    caps = []
+    for seed, lg_n, b, r in sample:
+        x = O.fill_field(seed, b << lg_n)
+        leaves = O.transpose_rev(O.batch_lde(x, lg_n, r, b), lg_n + r, b)
+        fill = O.ref_merkle_fill if O.ref_available() else O.merkle_fill
+        caps.append(fill(leaves, b, cap_height, 0)[1].reshape(-1, 4))
+    return caps
+
+
+def batched_section(args, zk, torch, baseline_legs: bool) -> dict:
+    """Config 3: 256 jobs, lg_n 12..20, polys 4..200, rate 1..3, cap height 4, Poseidon; inputs
+    fill_field(job_seed(3, j)), uniform in [0, p), resident on the device.  Arms, each over every job:
+    the plain per-job drop-in path of this library; zk_commit_batch per memory wave (autotuned); the
+    same waves as CUDA graphs; and (baseline leg) zeknox's own sm_100a build's per-job drop-in path."""
+    jobs = _jobs(0x5EED0003, args.batched_jobs, 12, 20, 4, 200, [1, 2, 3])
     ch = 4
-    pool = _device_pool(torch, max(b << lg for lg, b, _ in jobs), 0x5EED0003)
+    seeds = [job_seed(3, j) for j in range(len(jobs))]
+    offs = np.cumsum([0] + [b << lg for lg, b, _ in jobs])
+    inp = torch.empty(int(offs[-1]), dtype=torch.uint64, device="cuda")
+    views = []
+    for j, (lg, b, r) in enumerate(jobs):
+        v = inp[int(offs[j]): int(offs[j + 1])]
+        zk.fill_field(v, seeds[j])
+        views.append(v.view(b, 1 << lg))
     elems = sum(b << (lg + r) for lg, b, r in jobs)
     mx = max(b << (lg + r) for lg, b, r in jobs)
     mx_n = max(1 << (lg + r) for lg, b, r in jobs)
-    bufs = (torch.empty(mx, dtype=torch.uint64, device="cuda"), torch.empty(mx, dtype=torch.uint64, device="cuda"),
-            torch.empty(8 * mx_n, dtype=torch.uint64, device="cuda"), torch.empty(64, dtype=torch.uint64, device="cuda"))
-    zk.init_coset(0, 23, 7)
-    for lg, b, r in jobs[:4]:  # warm-up
-        _plain_job(zk, torch, pool[: b << lg], lg, r, b, ch, bufs)
+    max_lg = max(lg + r for lg, _, r in jobs)
+    res = {"workload": f"batched commit: {len(jobs)} jobs lg_n 12..20, polys 4..200, rate 1..3, cap_height 4, "
+                       "poseidon; inputs fill_field(job seed) resident on the device",
+           "jobs": len(jobs), "elems": elems}
+    # tables of every size first, for every arm (zeknox's are built by a serial kernel)
+    zk.init_coset(0, max_lg, 7)
+    for lg in sorted({lg + r for lg, _, r in jobs}):
+        zk.init_twiddle_factors(0, lg)
+    torch.cuda.synchronize()
+
+    # ---- plain per-job drop-in path of this library
+    plain = DropIn(torch, zk.capi.LIB, zk.capi.check, 0, mx, mx_n, mx)
+    for (lg, b, r), v in list(zip(jobs, views))[:4]:  # warm-up
+        plain.run(v.data_ptr(), lg, r, b, ch)
+    torch.cuda.synchronize()
+    caps_plain = []
     t0 = time.perf_counter()
-    for lg, b, r in jobs:
-        _plain_job(zk, torch, pool[: b << lg], lg, r, b, ch, bufs)
+    for (lg, b, r), v in zip(jobs, views):
+        caps_plain.append(plain.run(v.data_ptr(), lg, r, b, ch))
+    torch.cuda.synchronize()
     t_plain = time.perf_counter() - t0
-    del bufs
+    del plain
     torch.cuda.empty_cache()
-    # batched: waves of jobs whose outputs fit a budget
+
+    # ---- batched: waves of jobs whose outputs fit the budget, one zk_commit_batch each
     budget = args.budget_gb << 30
+    order = sorted(range(len(jobs)), key=lambda j: -(jobs[j][1] << (jobs[j][0] + jobs[j][2])))
     waves, cur, used = [], [], 0
-    for j in sorted(jobs, key=lambda j: -(j[1] << (j[0] + j[2]))):
-        need = (j[1] << (j[0] + j[2])) * 8 + (2 << (j[0] + j[2])) * 32
+    for j in order:
+        lg, b, r = jobs[j]
+        need = (b << (lg + r)) * 8 + (2 << (lg + r)) * 32
         if cur and used + need > budget:
             waves.append(cur)
             cur, used = [], 0
         cur.append(j)
         used += need
     waves.append(cur)
-    # the autotuner picks the LDE -> leaves plan of every shape class first
-    # (outside the timed region, like graph capture below)
     t0 = time.perf_counter()
-    tuned = sum(zk.autotune(lg, r, b) > 0 for lg, b, r in jobs)
+    tuned = sum(zk.autotune(lg, r, b) > 0 for lg, b, r in jobs)  # outside the timed region
     t_tune = time.perf_counter() - t0
-    # output buffers of a wave are allocated before its timed call (the plain
-    # path above reuses preallocated buffers too)
-    outs = []
-    t_batch = 0.0
+    caps_batch, caps_graph = [None] * len(jobs), [None] * len(jobs)
+    t_batch = t_graph = 0.0
     for wave in waves:
-        items = []
-        for lg, b, r in wave:
-            items.append((pool[: b << lg].view(b, 1 << lg), r, ch, 0, zk.CommitBuffers(1 << (lg + r), b, ch)))
+        items = [(views[j], jobs[j][2], ch, 0, zk.CommitBuffers(1 << (jobs[j][0] + jobs[j][2]), jobs[j][1], ch))
+                 for j in wave]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         zk.commit_batch(items, n_streams=args.streams)
         torch.cuda.synchronize()
         t_batch += time.perf_counter() - t0
-        outs.append(items[0][4].cap.cpu())
-        del items
-        torch.cuda.empty_cache()
-    # the same waves captured once into CUDA graphs (capture outside the timed
-    # region), each replayed as one graph launch
-    t_graph = 0.0
-    for wave in waves:
-        items = []
-        for lg, b, r in wave:
-            items.append((pool[: b << lg].view(b, 1 << lg), r, ch, 0, zk.CommitBuffers(1 << (lg + r), b, ch)))
+        for j, it in zip(wave, items):
+            caps_batch[j] = it[4].cap.cpu().numpy()
+            it[4].cap.zero_()
+        # the same wave captured once into a CUDA graph (capture outside the timed region), replayed
         g = zk.CommitGraph(items, n_streams=args.streams)
+        for it in items:
+            it[4].cap.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g.replay()
         torch.cuda.synchronize()
         t_graph += time.perf_counter() - t0
+        for j, it in zip(wave, items):
+            caps_graph[j] = it[4].cap.cpu().numpy()
         del g, items
         torch.cuda.empty_cache()
-    print(json.dumps({"workload": f"batched commit: {len(jobs)} jobs lg_n 12..20, polys 4..200, rate 1..3, "
-                                  "cap_height 4, poseidon",
-                      "elems": elems, "plain_per_job_elems_per_s": elems / t_plain,
-                      "batched_elems_per_s": elems / t_batch, "batched_over_plain": t_plain / t_batch,
-                      "graph_elems_per_s": elems / t_graph, "graph_over_plain": t_plain / t_graph,
-                      "autotuned_shape_classes": tuned, "autotune_s": t_tune,
-                      "plain_s": t_plain, "batched_s": t_batch, "waves": len(waves), "streams": args.streams,
-                      "budget_gb": args.budget_gb}), flush=True)
+    same = lambda a, b: all(np.array_equal(x.reshape(-1), y.reshape(-1)) for x, y in zip(a, b))  # noqa: E731
+    res.update({
+        "plain": {"elems_per_s": elems / t_plain, "s": t_plain,
+                  "path": "per job: compute_batched_lde -> compute_transpose_rev -> "
+                          "fill_digests_buf_linear_gpu_with_gpu_ptr -> cap D2H (this library, device buffers)"},
+        "batched": {"elems_per_s": elems / t_batch, "s": t_batch, "over_plain": t_plain / t_batch,
+                    "waves": len(waves), "streams": args.streams, "budget_gb": args.budget_gb,
+                    "autotuned_shape_classes": tuned, "autotune_s": t_tune},
+        "graph": {"elems_per_s": elems / t_graph, "s": t_graph, "over_plain": t_plain / t_graph},
+        "check": {"batched_caps_equal_plain": same(caps_batch, caps_plain),
+                  "graph_caps_equal_plain": same(caps_graph, caps_plain)},
+    })
+    if baseline_legs:
+        # zeknox's own sm_100a build, the same per-job drop-in calls on the same device inputs
+        ref = ref_gpu_build()
+        if ref is not None:
+            for lg in sorted({lg + r for lg, _, r in jobs}):
+                _check_rust(ref.init_twiddle_factors(0, lg))
+            _check_rust(ref.init_coset(0, max_lg, 7))
+            rp = DropIn(torch, ref, _check_rust, 0, mx, mx_n, mx)
+            for (lg, b, r), v in list(zip(jobs, views))[:4]:
+                rp.run(v.data_ptr(), lg, r, b, ch)
+            torch.cuda.synchronize()
+            caps_ref = []
+            t0 = time.perf_counter()
+            for (lg, b, r), v in zip(jobs, views):
+                caps_ref.append(rp.run(v.data_ptr(), lg, r, b, ch))
+            torch.cuda.synchronize()
+            t_ref = time.perf_counter() - t0
+            del rp
+            torch.cuda.empty_cache()
+            res["reference_gpu_plain"] = {
+                "elems_per_s": elems / t_ref, "s": t_ref,
+                "batched_over_it": t_ref / t_batch, "graph_over_it": t_ref / t_graph, "plain_over_it": t_ref / t_plain,
+                "build": "zeknox's CUDA sources compiled for sm_100a (oracle/_ref/libzkref_gpu.so), its per-job "
+                         "drop-in path on the same device inputs"}
+            res["check"]["plain_caps_equal_reference_gpu"] = same(caps_plain, caps_ref)
+        # a sample of the smallest jobs recomputed on the host
+        small = sorted(range(len(jobs)), key=lambda j: jobs[j][1] << (jobs[j][0] + jobs[j][2]))[: args.oracle_sample]
+        want = _oracle_caps([(seeds[j], jobs[j][0], jobs[j][1], jobs[j][2]) for j in small])
+        res["check"]["sample_caps_equal_oracle"] = same([caps_plain[j] for j in small], want)
+        res["check"]["oracle_sample"] = f"{len(small)} smallest jobs: host LDE + transpose by the oracle, Merkle " \
+                                        f"by zeknox's CPU path"
+    del inp, views
+    torch.cuda.empty_cache()
+    return res
 
 
-def run_served(args):
-    """Served stream: jobs lg_n 12..22, polys 8..300, rate 3, cap height 4, Poseidon, Poisson arrivals at
-    fractions of the plain path's capacity; the server (HBM budget, concurrent slots) vs a FIFO queue
-    served by the plain per-job drop-in path."""
+def served_section(args, zk, torch, baseline_legs: bool) -> dict:
+    """Config 5: the first `served_jobs` jobs of the seeded 10,000-job stream (lg_n 12..22, polys 8..300,
+    rate 3, cap height 4, Poseidon; inputs fill_field(job_seed(5, j)), generated on the device as each job
+    starts), Poisson arrivals at fractions of the plain path's capacity.
+
+    plain: the drop-in per-job path, one job at a time in arrival order (FIFO).  Each job's service time is
+    measured once, back to back in arrival order; the FIFO latencies at each rate follow from those times
+    and the arrival times (start = max(arrival, previous end)), or, with --served-replay, from a real-time
+    replay of the queue.  served: zk_server (120 GB budget, 4 slots), real time, seeded submissions."""
+    n_jobs = args.served_jobs
+    ch, r = 4, 3
+    jobs = _jobs(0x5EED0005, 10000, 12, 22, 8, 300, [3])[:n_jobs]
+    seeds = [job_seed(5, j) for j in range(n_jobs)]
+    elems = sum(b << (lg + r) for lg, b, _ in jobs)
+    mx_in = max(b << lg for lg, b, _ in jobs)
+    mx = max(b << (lg + r) for lg, b, _ in jobs)
+    mx_n = max(1 << (lg + r) for lg, _, _ in jobs)
+    zk.init_coset(0, max(lg for lg, _, _ in jobs) + r, 7)
+    for lg in sorted({lg + r for lg, _, _ in jobs}):
+        zk.init_twiddle_factors(0, lg)
+    dev_in = torch.empty(mx_in, dtype=torch.uint64, device="cuda")
+    # the LDE matrix of a job up to 60 GB; larger ones stream (leaves up to 80.5 GB beside it)
+    plain = DropIn(torch, zk.capi.LIB, zk.capi.check, mx_in, mx, mx_n, (60 << 30) // 8)
+
+    def plain_job(j):
+        lg, b, _ = jobs[j]
+        zk.fill_field(dev_in[: b << lg], seeds[j])
+        return plain.run(dev_in.data_ptr(), lg, r, b, ch)
+
+    plain_job(0)
+    torch.cuda.synchronize()
+    service, caps_plain = [], []
+    for j in range(n_jobs):
+        t0 = time.perf_counter()
+        caps_plain.append(plain_job(j))
+        service.append(time.perf_counter() - t0)
+    cap_jobs_per_s = n_jobs / sum(service)
+    rng = np.random.default_rng(0x5EED0055)
+    arrivals = {f: np.cumsum(rng.exponential(1.0 / (f * cap_jobs_per_s), n_jobs)) for f in args.served_rates}
+    res = {"workload": f"served: first {n_jobs} jobs of the seeded 10,000-job stream (lg_n 12..22, polys 8..300, "
+                       "rate 3, cap_height 4, poseidon); inputs fill_field(job seed) generated on the device at "
+                       "each job's start (both arms)",
+           "jobs": n_jobs, "elems": elems, "plain_capacity_jobs_per_s": cap_jobs_per_s,
+           "plain_capacity_elems_per_s": elems / sum(service), "plain_streamed_jobs": plain.streamed,
+           "plain_service_s": {"p50": _pct(service, 50), "p99": _pct(service, 99), "max": max(service)},
+           "slots": args.streams, "budget_gb": args.budget_gb, "rates": {}}
+
+    replay = {}
+    if args.served_replay:
+        for f in args.served_rates:
+            lat = []
+            t0 = time.perf_counter()
+            for j, a in enumerate(arrivals[f]):
+                now = time.perf_counter() - t0
+                if now < a:
+                    time.sleep(a - now)
+                plain_job(j)
+                lat.append(time.perf_counter() - t0 - a)
+            replay[f] = (lat, time.perf_counter() - t0 - arrivals[f][0])
+    del plain, dev_in
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    all_caps_ok = True
+    for f in args.served_rates:
+        lat_p, span_p = replay[f] if f in replay else fifo_latencies(arrivals[f], service)
+        runs = []
+        for rep in range(args.served_repeats):
+            with zk.Server(hbm_budget_bytes=args.budget_gb << 30, slots=args.streams) as srv:
+                lat_s, caps_s, errs = {}, {}, []
+                tick = {}
+
+                def client():  # completions in order; each tree released at once
+                    try:
+                        while len(lat_s) < n_jobs:
+                            t = srv.wait_any(timeout_ms=1000)
+                            if t is not None:
+                                cap, lat = srv.wait(t)
+                                lat_s[t], caps_s[t] = lat, cap
+                                srv.release(t)
+                    except Exception as e:  # noqa: BLE001 - reported by the main thread
+                        errs.append(e)
+
+                th = threading.Thread(target=client)
+                th.start()
+                t0 = time.perf_counter()
+                for j, a in enumerate(arrivals[f]):
+                    now = time.perf_counter() - t0
+                    if now < a:
+                        time.sleep(a - now)
+                    lg, b, _ = jobs[j]
+                    tick[j] = srv.submit_seeded(seeds[j], lg, b, r, ch)
+                th.join()
+                if errs:
+                    raise errs[0]
+                span = time.perf_counter() - t0 - arrivals[f][0]
+                st = srv.stats()
+            ok = all(np.array_equal(caps_s[tick[j]].reshape(-1), caps_plain[j].reshape(-1)) for j in range(n_jobs))
+            all_caps_ok &= ok
+            lats = [lat_s[tick[j]] for j in range(n_jobs)]
+            runs.append({"p50_s": _pct(lats, 50), "p99_s": _pct(lats, 99), "elems_per_s": elems / span,
+                         "late_jobs": st["late"], "max_queue": st["max_queue"],
+                         "hbm_peak_gb": st["hbm_peak"] / 2**30})
+        med = lambda k: float(np.median([x[k] for x in runs]))  # noqa: E731
+        entry = {
+            "arrival_jobs_per_s": f * cap_jobs_per_s,
+            "plain": {"p50_s": _pct(lat_p, 50), "p99_s": _pct(lat_p, 99), "elems_per_s": elems / span_p,
+                      "how": "real-time replay" if f in replay else "FIFO over measured service times"},
+            "served": {"p50_s": med("p50_s"), "p99_s": med("p99_s"), "elems_per_s": med("elems_per_s"),
+                       "late_jobs": int(med("late_jobs")), "max_queue": int(med("max_queue")),
+                       "hbm_peak_gb": med("hbm_peak_gb")},
+        }
+        if len(runs) > 1:
+            entry["served"]["runs"] = runs
+        entry["served_over_plain"] = {"p50": entry["plain"]["p50_s"] / entry["served"]["p50_s"],
+                                      "p99": entry["plain"]["p99_s"] / entry["served"]["p99_s"],
+                                      "elems_per_s": entry["served"]["elems_per_s"] / entry["plain"]["elems_per_s"]}
+        res["rates"][str(f)] = entry
+        print(json.dumps({"rate": f, **entry}), file=sys.stderr, flush=True)
+    res["check"] = {"served_caps_equal_plain": bool(all_caps_ok)}
+    if baseline_legs:
+        small = sorted(range(n_jobs), key=lambda j: jobs[j][1] << jobs[j][0])[: args.oracle_sample]
+        want = _oracle_caps([(seeds[j], jobs[j][0], jobs[j][1], r) for j in small])
+        res["check"]["sample_caps_equal_oracle"] = all(np.array_equal(caps_plain[j].reshape(-1), w.reshape(-1))
+                                                       for j, w in zip(small, want))
+    return res
+
+
+def run_batched(args):
     import torch
 
     import zeknox_b200 as zk
 
-    n_jobs = args.jobs or 40
-    ch, r = 4, 3
-    stream = _jobs(0x5EED0005, 10000, 12, 22, 8, 300, [3])  # the seeded 10,000-job stream
-    # The drop-in path holds the LDE matrix and the leaves (2 x 8 B per point): keep the first jobs for
-    # which that fits next to the input in HBM, so both paths run the same jobs.
-    jobs = [j for j in stream if (j[1] << (j[0] + r)) * 16 + (j[1] << j[0]) * 8 <= 140 << 30][:n_jobs]
-    mx_in = max(b << lg for lg, b, _ in jobs)
-    mx = max(b << (lg + r) for lg, b, _ in jobs)
-    mx_n = max(1 << (lg + r) for lg, _, _ in jobs)
-    host = torch.empty(mx_in, dtype=torch.uint64).pin_memory()
-    host.view(torch.int64).copy_(_device_pool(torch, mx_in, 0x5EED0005).view(torch.int64).cpu())
-    zk.init_coset(0, 25, 7)
-    dev_in = torch.empty(mx_in, dtype=torch.uint64, device="cuda")
-    bufs = (torch.empty(mx, dtype=torch.uint64, device="cuda"), torch.empty(mx, dtype=torch.uint64, device="cuda"),
-            torch.empty(8 * mx_n, dtype=torch.uint64, device="cuda"), torch.empty(64, dtype=torch.uint64, device="cuda"))
+    print(json.dumps(batched_section(args, zk, torch, not args.no_cpu_baseline)), flush=True)
 
-    def plain(lg, b):  # host coefficients in, as a served request would arrive
-        dev_in[: b << lg].copy_(host[: b << lg])
-        _plain_job(zk, torch, dev_in[: b << lg], lg, r, b, ch, bufs)
 
-    plain(*jobs[0][:2])
-    service = []
-    for lg, b, _ in jobs:
-        t0 = time.perf_counter()
-        plain(lg, b)
-        service.append(time.perf_counter() - t0)
-    cap_jobs_per_s = n_jobs / sum(service)
-    elems = sum(b << (lg + r) for lg, b, _ in jobs)
-    res = {"workload": f"served: {n_jobs} jobs of the seeded 10,000-job stream (lg_n 12..22, polys 8..300, "
-                       "rate 3, cap_height 4, poseidon; jobs whose drop-in path fits in HBM)",
-           "plain_capacity_jobs_per_s": cap_jobs_per_s, "plain_capacity_elems_per_s": elems / sum(service),
-           "slots": args.streams, "budget_gb": args.budget_gb, "rates": {}}
-    rng = np.random.default_rng(0x5EED0055)
-    arrivals = {f: np.cumsum(rng.exponential(1.0 / (f * cap_jobs_per_s), n_jobs)) for f in args.rates}
-    # plain path first: one FIFO queue, one job per call, in real time
-    plain_res = {}
-    for f in args.rates:
-        lat = []
-        t0 = time.perf_counter()
-        for a, (lg, b, _) in zip(arrivals[f], jobs):
-            now = time.perf_counter() - t0
-            if now < a:
-                time.sleep(a - now)
-            plain(lg, b)
-            lat.append(time.perf_counter() - t0 - a)
-        plain_res[f] = (lat, time.perf_counter() - t0)
-    # free the plain path's buffers: the server owns the HBM budget from here
-    del bufs, dev_in
-    torch.cuda.synchronize()
-    torch.cuda.empty_cache()
-    import threading
+def run_served(args):
+    import torch
 
-    for f in args.rates:
-        with zk.Server(hbm_budget_bytes=args.budget_gb << 30, slots=args.streams) as srv:
-            lat_s, errs = [], []
+    import zeknox_b200 as zk
 
-            def client():  # collects jobs in completion order and releases their trees at once
-                try:
-                    while len(lat_s) < len(jobs):
-                        t = srv.wait_any(timeout_ms=1000)
-                        if t is not None:
-                            lat_s.append(srv.wait(t)[1])
-                            srv.release(t)
-                except Exception as e:  # noqa: BLE001 - reported by the main thread
-                    errs.append(e)
+    print(json.dumps(served_section(args, zk, torch, not args.no_cpu_baseline)), flush=True)
 
-            th = threading.Thread(target=client)
-            th.start()
-            t0 = time.perf_counter()
-            for a, (lg, b, _) in zip(arrivals[f], jobs):
-                now = time.perf_counter() - t0
-                if now < a:
-                    time.sleep(a - now)
-                srv.submit(host[: b << lg].view(b, 1 << lg), r, ch, 0)
-            th.join()
-            if errs:
-                raise errs[0]
-            span_srv = time.perf_counter() - t0
-            st = srv.stats()
-        lat, span_plain = plain_res[f]
-        res["rates"][str(f)] = {
-            "arrival_jobs_per_s": f * cap_jobs_per_s,
-            "plain": {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-                      "elems_per_s": elems / span_plain},
-            "served": {"p50_s": float(np.percentile(lat_s, 50)), "p99_s": float(np.percentile(lat_s, 99)),
-                       "elems_per_s": elems / span_srv, "max_queue": st["max_queue"],
-                       "hbm_peak_gb": st["hbm_peak"] / 2**30},
-        }
-        print(json.dumps({"rate": f, **res["rates"][str(f)]}), flush=True)
-    print(json.dumps(res), flush=True)
 
 if __name__ == "__main__":
     main()

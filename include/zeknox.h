@@ -139,6 +139,12 @@ ZK_EXTERN RustError zk_last_error(void);
 /* Number of kernels this library has launched in this process. */
 ZK_EXTERN uint64_t zk_kernel_launches(void);
 
+/* count field elements uniform in [0, p) from seed, stream-ordered, into
+ * d_out: element i is the first z(seed, i + j * count), j = 0, 1, ..., below p,
+ * z(s, c) = SplitMix64's output function of s + (c + 1) * 0x9E3779B97F4A7C15
+ * (the stream of the salt rows).  Synthetic inputs for tests and benchmarks. */
+ZK_EXTERN RustError zk_fill_field_async(void *d_out, uint64_t count, uint64_t seed, void *stream);
+
 /* Stream-ordered variants for callers that manage their own CUDA streams
  * (device pointers only, no synchronisation; `stream` is a cudaStream_t). */
 ZK_EXTERN RustError zk_lde_async(void *d_output, const void *d_input, uint32_t lg_n, uint32_t rate_bits,
@@ -188,15 +194,18 @@ ZK_EXTERN RustError zk_merkle_async(void *d_digests, void *d_cap, const void *d_
                                     uint64_t hash_type, void *stream);
 
 /* Allocation-free coset LDE (no counterpart in zeknox).  Same arguments and
- * result as zk_lde_async (device buffers, stream-ordered, coset generator 7)
- * for callers that cannot call cudaMalloc at this point: work captured into a
- * CUDA graph, provers confined to a pre-reserved memory budget or arena, hot
- * paths where allocation is forbidden.  Its NTT intermediate and tables live in
- * one static device array (32 MiB + 96 KiB per GPU, held until exit), so:
- * lg_n + rate_bits must be <= 22 (else code cudaErrorMemoryAllocation = 2,
- * NULL message); calls that overlap on the GPU race on the shared array; the
- * first call on a device resolves the array's address (make it before any
- * stream capture).  Errors never carry a message (nothing is allocated). */
+ * result as zk_lde_async (device buffers, stream-ordered, the installed coset
+ * generator: 7 unless init_coset set another) for callers that cannot call
+ * cudaMalloc where they run it: provers confined to a pre-reserved memory
+ * budget or their own arena (the regular entry points grow the CUDA memory
+ * pool), and hot paths where allocation calls are forbidden because they can
+ * synchronise the device.  Its NTT intermediate and tables live in one static
+ * device array (32 MiB + 96 KiB per GPU, held until exit), so: lg_n +
+ * rate_bits must be <= 22 (else code cudaErrorMemoryAllocation = 2, NULL
+ * message); calls that overlap on the GPU race on the shared array; the first
+ * call on a device resolves the array's address (make it before any stream
+ * capture).  Returned errors never carry a message; a CUDA failure inside the
+ * transform is also recorded, with its text, for zk_last_error(). */
 ZK_EXTERN RustError zk_lde_noalloc(void *d_output, const void *d_input, uint32_t lg_n, uint32_t rate_bits,
                                    uint32_t batches, uint32_t inv, uint32_t with_coset, void *stream);
 
@@ -232,7 +241,11 @@ ZK_EXTERN RustError zk_autotune_reset(void);
  * caller until the job completes), admitted onto n_slots concurrent streams
  * while leaves + digests + cap of resident trees plus coefficients + scratch of
  * running jobs fit hbm_budget_bytes, and keep their tree on the device until
- * released.  zk_server_wait blocks until the cap is on the host.
+ * released.  Admission keeps each job within the completion time a FIFO queue
+ * served one job at a time would give it (estimated from job sizes), plus a
+ * tenth of its own estimated GPU time; later, shorter jobs run ahead of or
+ * beside earlier ones only inside that slack.
+ * zk_server_wait blocks until the cap is on the host.
  * zk_server_wait_any returns, in completion order, each job that has finished
  * (or failed) since the last call, once; *ticket = 0 when nothing is pending or
  * when timeout_ms passes first (UINT32_MAX waits without limit).  The server
@@ -243,16 +256,30 @@ typedef struct {
     double p50_s, p99_s, max_s; /* submit -> cap on the host */
     double elems, elems_per_s;  /* committed LDE evaluations; first submit -> last completion */
     uint64_t hbm_in_use, hbm_peak;
+    uint64_t late; /* completed jobs that finished after their estimated FIFO completion plus slack */
 } ZkServerStats;
 ZK_EXTERN RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes, uint32_t n_slots, ZkServer **out);
 ZK_EXTERN RustError zk_server_submit(ZkServer *srv, const void *host_coeffs, uint32_t lg_n, uint32_t rate_bits,
                                      uint32_t batches, uint32_t cap_height, uint32_t hash_type, uint64_t *ticket);
+/* A job whose coefficients (batches x 2^lg_n) are the field-element stream
+ * zk_fill_field_async(seed) writes, generated on the device when the job is
+ * admitted instead of copied from the host: a load source for measuring the
+ * server with device-resident inputs. */
+ZK_EXTERN RustError zk_server_submit_seeded(ZkServer *srv, uint64_t seed, uint32_t lg_n, uint32_t rate_bits,
+                                            uint32_t batches, uint32_t cap_height, uint32_t hash_type,
+                                            uint64_t *ticket);
 ZK_EXTERN RustError zk_server_wait(ZkServer *srv, uint64_t ticket, uint64_t *host_cap, double *latency_s);
 ZK_EXTERN RustError zk_server_wait_any(ZkServer *srv, uint32_t timeout_ms, uint64_t *ticket);
 ZK_EXTERN RustError zk_server_result(ZkServer *srv, uint64_t ticket, void **d_leaves, void **d_digests,
                                      void **d_cap);
 ZK_EXTERN RustError zk_server_release(ZkServer *srv, uint64_t ticket);
 ZK_EXTERN RustError zk_server_stats(ZkServer *srv, ZkServerStats *out);
+/* Host-side fault injection for tests: the next n_jobs admitted jobs fail at
+ * their at_allocation-th device allocation (1 = coefficients, 2 = leaves,
+ * 3 = digests, ...) as if the pool were exhausted.  A failed job reports its
+ * error through zk_server_wait; its partial allocations are freed and the
+ * server keeps serving. */
+ZK_EXTERN RustError zk_server_inject_failure(ZkServer *srv, uint32_t n_jobs, uint32_t at_allocation);
 ZK_EXTERN RustError zk_server_destroy(ZkServer *srv);
 
 #endif /* ZEKNOX_B200_H */

@@ -9,11 +9,17 @@
 #                                reference GPU build the -m gpu tests compare against.
 #
 # The sources are compiled where they lie; nothing is copied into this repo.
-# Outputs go to oracle/_ref/ only.  Needs the zeknox tree (default
-# /root/reference); on a machine without it this script does nothing.
+# Outputs go to oracle/_ref/ only.  Needs the zeknox tree, named by the
+# ZEKNOX_SRC environment variable or the first argument; without it (or on a
+# machine without the tree) this script does nothing.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-SRC="${ZEKNOX_SRC:-/root/reference}/native"
+ROOT_SRC="${1:-${ZEKNOX_SRC:-}}"
+if [ -z "$ROOT_SRC" ]; then
+    echo "build_ref: set ZEKNOX_SRC (or pass the zeknox tree as the first argument); skipping" >&2
+    exit 0
+fi
+SRC="$ROOT_SRC/native"
 OUT="$HERE/_ref"
 if [ ! -d "$SRC" ]; then
     echo "build_ref: zeknox sources not found at $SRC; skipping" >&2

@@ -110,6 +110,26 @@ def field_elems(seed: int, n: int) -> np.ndarray:
     return np.ascontiguousarray(out[:n])
 
 
+def fill_field(seed: int, n: int) -> np.ndarray:
+    """The product's synthetic-input stream (zk_fill_field_async, the salt rows'
+    generator, ntt.cu salt_kernel), restated: element i is the first
+    z(seed, i + j n), j = 0, 1, ..., below p, with z(s, c) = SplitMix64's
+    output function of s + (c + 1) * 0x9E3779B97F4A7C15."""
+    out = np.empty(n, dtype=np.uint64)
+    todo = np.arange(n, dtype=np.uint64)
+    ctr = todo.copy()
+    while todo.size:
+        with np.errstate(over="ignore"):
+            z = np.uint64(seed) + (ctr + np.uint64(1)) * np.uint64(0x9E3779B97F4A7C15)
+            z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+            z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+            z = z ^ (z >> np.uint64(31))
+        ok = z < np.uint64(P)
+        out[todo[ok]] = z[ok]
+        todo, ctr = todo[~ok], ctr[~ok] + np.uint64(n)
+    return out
+
+
 # ---------------------------------------------------------------- hashing
 def hash_one(ht: int, leaf: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
     leaf = np.ascontiguousarray(leaf, dtype=np.uint64)

@@ -20,6 +20,7 @@ Usage: python tests/golden/make_golden.py [zeknox-root]
 """
 
 import json
+import os
 import re
 import sys
 from pathlib import Path
@@ -103,7 +104,10 @@ def merkle_fixtures() -> dict:
 
 
 def main():
-    zk = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ZEKNOX_SRC")
+    if not src:
+        sys.exit("usage: make_golden.py <zeknox source tree>   (or set ZEKNOX_SRC)")
+    zk = Path(src)
     here = Path(__file__).resolve().parent
     (here / "kat.json").write_text(json.dumps(parse_kats(zk), indent=1) + "\n")
     np.savez_compressed(here / "merkle_ref_cpu.npz", **merkle_fixtures())

@@ -142,22 +142,96 @@ def test_server_wait_any_returns_each_job_once(zk, oracle):
         assert srv.stats()["hbm_in_use"] == 0
 
 
-def test_server_large_job_lane_is_fifo(zk, oracle, monkeypatch):
-    """With every job in the large-job lane (threshold 0 s), jobs run one at a
-    time in arrival order: completions come back in submission order."""
+def test_server_equal_jobs_submitted_together_run_in_fifo_order(zk, oracle):
+    """Jobs of one size submitted together leave one another no slack past
+    their FIFO finish times: they run one at a time in arrival order, so
+    completions come back in submission order."""
     import torch
 
-    monkeypatch.setenv("ZK_SERVER_BIG_JOB_S", "0")
-    jobs = _mixed_jobs(oracle, 8, 29)
-    want = [zk.commit(_dev(x), r, ch, ht).cap.cpu().numpy() for x, r, ch, ht in jobs]
+    x = oracle.field_elems(2929, 24 << 13).reshape(24, 1 << 13)
+    want = zk.commit(_dev(x), 3, 4, 0).cap.cpu().numpy()
     torch.cuda.synchronize()
     with zk.Server(hbm_budget_bytes=4 << 30, slots=4) as srv:
-        tickets = [srv.submit(x, r, ch, ht) for x, r, ch, ht in jobs]
-        order = [srv.wait_any(timeout_ms=60000) for _ in jobs]
+        tickets = [srv.submit(x, 3, 4, 0) for _ in range(8)]
+        order = [srv.wait_any(timeout_ms=60000) for _ in tickets]
         assert order == tickets
-        for t, w in zip(tickets, want):
-            assert np.array_equal(srv.wait(t)[0], w)
+        for t in tickets:
+            assert np.array_equal(srv.wait(t)[0], want)
             srv.release(t)
+        assert srv.stats()["hbm_in_use"] == 0
+
+
+def test_server_short_job_runs_beside_a_long_one(zk, oracle):
+    """A short job submitted right behind a long one fits in the long job's
+    slack: it is admitted at once, beside it, and finishes first."""
+    with zk.Server(hbm_budget_bytes=16 << 30, slots=4) as srv:
+        big = srv.submit_seeded(11, 20, 64, 3, 4)   # 64 x 2^20 -> 2^23 leaves: tens of ms
+        small = srv.submit_seeded(12, 8, 4, 1, 2)   # 4 x 2^8 -> 2^9 leaves
+        first = srv.wait_any(timeout_ms=60000)
+        second = srv.wait_any(timeout_ms=60000)
+        assert (first, second) == (small, big)
+        for t in (big, small):
+            srv.wait(t)
+            srv.release(t)
+
+
+def test_fill_field_matches_the_oracle_stream(zk, oracle):
+    import torch
+
+    out = torch.empty(100003, dtype=torch.uint64, device="cuda")
+    zk.fill_field(out, 0x5EED0005)
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), oracle.fill_field(0x5EED0005, 100003))
+
+
+def test_server_seeded_jobs_equal_commits_of_their_inputs(zk, oracle):
+    """A seeded job commits fill_field(seed) generated on the device at
+    admission: its cap equals the commit of that input made alone, and (small
+    shapes) the oracle's commit of the same stream."""
+    import torch
+
+    shapes = [(9, 2, 17, 2), (12, 3, 40, 4), (15, 1, 9, 4), (10, 3, 135, 3), (14, 2, 200, 4)]
+    with zk.Server(hbm_budget_bytes=4 << 30, slots=4) as srv:
+        tickets = [srv.submit_seeded(7000 + k, lg_n, b, r, ch) for k, (lg_n, r, b, ch) in enumerate(shapes)]
+        for k, ((lg_n, r, b, ch), t) in enumerate(zip(shapes, tickets)):
+            cap, _ = srv.wait(t)
+            x = torch.empty((b, 1 << lg_n), dtype=torch.uint64, device="cuda")
+            zk.fill_field(x, 7000 + k)
+            alone = zk.commit(x, r, ch, 0).cap.cpu().numpy()
+            assert np.array_equal(cap, alone)
+            if b << lg_n <= 1 << 16:
+                xs = oracle.fill_field(7000 + k, b << lg_n)
+                leaves = oracle.transpose_rev(oracle.batch_lde(xs, lg_n, r, b), lg_n + r, b)
+                _, want = oracle.merkle_fill(leaves, b, ch, oracle.HASH_POSEIDON)
+                assert np.array_equal(cap.reshape(-1), want)
+            srv.release(t)
+
+
+@pytest.mark.parametrize("at_allocation", [1, 2, 4])
+def test_server_injected_allocation_failure_frees_and_keeps_serving(zk, oracle, at_allocation):
+    """Host-side fault injection: one job's at_allocation-th device allocation
+    fails.  That job reports the error; what it had allocated is freed and its
+    budget returned (hbm_in_use back to 0), and the jobs around it complete
+    with the caps they have alone."""
+    import torch
+
+    jobs = [(9, 3, 20, 2), (11, 2, 33, 3), (10, 3, 7, 4), (12, 1, 60, 4)]
+    with zk.Server(hbm_budget_bytes=1 << 30, slots=2) as srv:
+        first = srv.submit_seeded(8100, jobs[0][0], jobs[0][2], jobs[0][1], jobs[0][3])
+        srv.wait(first)
+        srv.inject_failure(1, at_allocation)
+        tickets = [srv.submit_seeded(8101 + k, lg_n, b, r, ch) for k, (lg_n, r, b, ch) in enumerate(jobs[1:])]
+        with pytest.raises(zk.ZeknoxError, match="injected allocation failure"):
+            srv.wait(tickets[0])
+        for k, t in enumerate(tickets[1:], start=1):
+            lg_n, r, b, ch = jobs[k + 1]
+            x = torch.empty((b, 1 << lg_n), dtype=torch.uint64, device="cuda")
+            zk.fill_field(x, 8101 + k)
+            assert np.array_equal(srv.wait(t)[0], zk.commit(x, r, ch, 0).cap.cpu().numpy())
+        for t in [first, *tickets]:
+            srv.release(t)
+        st = srv.stats()
+        assert st["hbm_in_use"] == 0 and st["completed"] == 3
 
 
 def test_commit_batch_graph_replays_bit_exact(zk, oracle):

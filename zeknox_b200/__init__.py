@@ -215,6 +215,21 @@ class Server:
         self._keep[t.value] = (host_coeffs, cap_height)
         return t.value
 
+    def submit_seeded(self, seed: int, lg_n: int, batches: int, rate_bits: int, cap_height: int,
+                      hash_type: int = HashPoseidon) -> int:
+        """A job whose (batches, 2^lg_n) coefficients are fill_field(seed), generated on the device at admission."""
+        import ctypes
+
+        t = ctypes.c_uint64()
+        capi.check(capi.LIB.zk_server_submit_seeded(self._h, seed, lg_n, rate_bits, batches, cap_height, hash_type,
+                                                    ctypes.byref(t)))
+        self._keep[t.value] = (None, cap_height)
+        return t.value
+
+    def inject_failure(self, n_jobs: int, at_allocation: int):
+        """Test hook: the next n_jobs admitted jobs fail at their at_allocation-th device allocation."""
+        capi.check(capi.LIB.zk_server_inject_failure(self._h, n_jobs, at_allocation))
+
     def wait(self, ticket: int):
         """-> (cap as a (2^cap_height, 4) uint64 array, latency in seconds)."""
         import ctypes
@@ -265,6 +280,15 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def fill_field(out, seed: int, stream=None):
+    """Fill a uint64 CUDA tensor with field elements uniform in [0, p) from `seed` (zk_fill_field_async)."""
+    import torch
+
+    assert out.dtype == torch.uint64 and out.is_cuda and out.is_contiguous()
+    capi.check(capi.LIB.zk_fill_field_async(out.data_ptr(), out.numel(), seed & (2**64 - 1), _stream_ptr(stream)))
+    return out
 
 
 def merkle_sizes(n_leaves: int, cap_height: int):

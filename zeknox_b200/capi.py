@@ -79,7 +79,7 @@ class ZkServerStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_uint64), ("queued", ctypes.c_uint64), ("max_queue", ctypes.c_uint64),
                 ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("max_s", ctypes.c_double),
                 ("elems", ctypes.c_double), ("elems_per_s", ctypes.c_double), ("hbm_in_use", ctypes.c_uint64),
-                ("hbm_peak", ctypes.c_uint64)]
+                ("hbm_peak", ctypes.c_uint64), ("late", ctypes.c_uint64)]
 
 
 assert ctypes.sizeof(NTTConfig) == 24 and ctypes.sizeof(TransposeConfig) == 8
@@ -128,6 +128,9 @@ def _load() -> ctypes.CDLL:
         "zk_server_release": (RustError, [vp, u64]),
         "zk_server_stats": (RustError, [vp, ctypes.POINTER(ZkServerStats)]),
         "zk_server_destroy": (RustError, [vp]),
+        "zk_server_submit_seeded": (RustError, [vp, u64, u32, u32, u32, u32, u32, ctypes.POINTER(u64)]),
+        "zk_server_inject_failure": (RustError, [vp, u32, u32]),
+        "zk_fill_field_async": (RustError, [vp, u64, u64, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

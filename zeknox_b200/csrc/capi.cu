@@ -24,6 +24,17 @@ namespace {
 thread_local int t_last_code = 0;
 thread_local std::string t_last_msg;
 
+}  // namespace
+
+namespace zk {
+void record_last_error(int code, const char *msg) {
+    t_last_code = code;
+    t_last_msg = msg ? msg : "";
+}
+}  // namespace zk
+
+namespace {
+
 RustError make_error(int code, const char *msg) {
     RustError r;
     r.code = code;
@@ -52,8 +63,7 @@ template <class F>
 void guarded_void(F &&f) {
     RustError r = guarded(f);
     if (r.code) {
-        t_last_code = r.code;
-        t_last_msg = r.message ? r.message : "";
+        zk::record_last_error(r.code, r.message);
         fprintf(stderr, "zeknox-b200: %s\n", t_last_msg.c_str());
     }
     free(r.message);
@@ -458,6 +468,13 @@ extern "C" RustError zk_last_error(void) {
 }
 
 extern "C" uint64_t zk_kernel_launches(void) { return launch_count(); }
+
+extern "C" RustError zk_fill_field_async(void *d_out, uint64_t count, uint64_t seed, void *stream) {
+    return guarded([&] {
+        require(d_out != nullptr || count == 0, "null buffer");
+        salt_run((uint64_t *)d_out, count, seed, (cudaStream_t)stream);
+    });
+}
 
 extern "C" RustError zk_lde_async(void *d_output, const void *d_input, uint32_t lg_n, uint32_t rate_bits,
                                  uint32_t batches, uint32_t inv, uint32_t with_coset, void *stream) {

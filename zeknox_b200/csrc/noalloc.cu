@@ -1,13 +1,14 @@
-// zk_lde_noalloc: the coset LDE with no device (or host) allocation at all.
+// zk_lde_noalloc: the coset LDE with no device allocation.
 //
-// Who needs it: callers that cannot call cudaMalloc at the point where they
-// run the LDE -- code being captured into a CUDA graph (allocation calls are
-// not capturable), provers that run inside a fixed, pre-reserved memory
-// budget or a custom arena and must not let a library grow the CUDA memory
-// pool behind their back, and embedders that forbid allocation on their hot
-// path for latency reasons.  The regular entry points allocate the NTT
-// intermediate and the twiddle / coset tables on demand; this one keeps all of
-// them in one file-scope device array of fixed size instead.
+// Who needs it: callers that cannot call cudaMalloc where they run the LDE.
+// Provers that run inside a fixed, pre-reserved memory budget or their own
+// arena must not let a library grow the CUDA memory pool behind their back
+// (the regular entry points allocate the NTT intermediate and the twiddle /
+// coset tables on demand, and the pool keeps that memory); embedders with
+// hard latency limits forbid allocation calls on their hot path, because
+// cudaMalloc can synchronise the device and take milliseconds.  This entry
+// point keeps its intermediate and tables in one file-scope device array of
+// fixed size instead.
 //
 // Limits and sharing rules:
 //  * the array holds 2^22 elements of NTT intermediate (32 MiB) plus the
@@ -16,12 +17,19 @@
 //  * transforms up to 2^22 points (lg_n + rate_bits <= 22) are accepted;
 //    larger ones are rejected with code cudaErrorMemoryAllocation (2) and a
 //    NULL message (the message is not allocated either);
-//  * every call reuses the same array and leaves its contents behind; calls
-//    whose work overlaps on the GPU (different streams, or different host
-//    threads) race on it and must be serialised by the caller;
+//  * every call reuses the same array and leaves its contents behind (its
+//    tables are rewritten by each call, and its intermediate is fully written
+//    before it is read); calls whose work overlaps on the GPU (different
+//    streams, or different host threads) race on it and must be serialised by
+//    the caller;
 //  * the first call on a device resolves the array's device address
 //    (cudaGetSymbolAddress, which also loads this module on that device); make
-//    that first call before any stream capture on the device.
+//    that first call before any stream capture on the device;
+//  * the coset is the one the device's coset LDEs use: generator 7, or the one
+//    init_coset installed last;
+//  * a CUDA failure inside the transform (a launch error) is raised and caught
+//    internally; that path allocates host memory for the error text, which
+//    zk_last_error() then returns.  Argument and size errors allocate nothing.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -97,8 +105,10 @@ extern "C" RustError zk_lde_noalloc(void *d_output, const void *d_input, uint32_
     uint64_t *scratch = base, *line = base + kScratchElems, *roots_dev = line + kLineElems,
              *coset_dev = roots_dev + kPowElems;
 
-    // Tables for this call (same values as the cached tables of the regular path).
+    // Tables for this call: the same values as the cached tables of the regular
+    // path, coset generator included.
     const bool inverse = inv != 0;
+    const uint64_t gen = zk::installed_coset_generator(dev);
     uint64_t w4096 = zk::h_omega(zk::kLineLgMax), wn = zk::h_omega(lg);
     if (inverse) {
         w4096 = zk::h_inv(w4096);
@@ -112,13 +122,22 @@ extern "C" RustError zk_lde_noalloc(void *d_output, const void *d_input, uint32_
     cos.dev = coset_dev;
     cos.bits = lg;
     cos.h = (lg + 1) / 2;
-    cos.base = zk::GROUP_GENERATOR;
+    cos.base = gen;
     const uint64_t lo_n = 1ull << roots.h, hi_n = 1ull << (lg - roots.h);
+    // Each launch is checked and counted like every other launch of the library.
+    auto launched = [] {
+        const cudaError_t le = cudaGetLastError();
+        if (le == cudaSuccess) zk::note_launch();
+        return le;
+    };
     fill_pow_table<<<16, 256, 0, s>>>(line, w4096, kLineElems, 0);
+    if ((e = launched()) != cudaSuccess) return err(-(int)e);
     fill_pow_table<<<8, 256, 0, s>>>(roots_dev, wn, lo_n, hi_n);
-    if (with_coset) fill_pow_table<<<8, 256, 0, s>>>(coset_dev, zk::GROUP_GENERATOR, lo_n, hi_n);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return err(-(int)e);
+    if ((e = launched()) != cudaSuccess) return err(-(int)e);
+    if (with_coset) {
+        fill_pow_table<<<8, 256, 0, s>>>(coset_dev, gen, lo_n, hi_n);
+        if ((e = launched()) != cudaSuccess) return err(-(int)e);
+    }
 
     zk::NttJob j;
     j.src = (const uint64_t *)d_input;
@@ -136,7 +155,11 @@ extern "C" RustError zk_lde_noalloc(void *d_output, const void *d_input, uint32_
     try {
         zk::ntt_run_on_tables(j, roots, line, s);
     } catch (const zk::Error &ex) {
+        zk::record_last_error(ex.code, ex.what());
         return err(ex.code);
+    } catch (const std::exception &ex) {
+        zk::record_last_error(-(int)cudaErrorUnknown, ex.what());
+        return err(-(int)cudaErrorUnknown);
     }
     return err(0);
 }

@@ -692,28 +692,20 @@ Plan plan_with_passes(uint32_t lg, int passes) {
 // 160 KB of dynamic shared memory the pass launches with.
 bool leaves_fits(uint32_t l, uint32_t lg_t) { return pass_smem(l, lg_t) <= 160 * 1024; }
 
-// One batched transform of `batches` polynomials of 2^lg elements.
-void ntt_run(const NttJob &j, cudaStream_t s) {
-    const uint32_t lg = j.lg;
-    require(lg >= 1 && lg <= 32, "transform size out of range");
-    if (j.batches == 0) return;
-    DeviceCtx &ctx = device_ctx(current_device());
-    const PowTable &rt = root_table(ctx, lg, j.inverse);
-    const uint64_t *lr = line_roots(ctx, j.inverse);
-    const LeavesChoice tuned = j.to_leaves ? leaves_choice(lg, j.batches) : LeavesChoice{};
-    const Plan plan = tuned.passes ? plan_with_passes(lg, tuned.passes) : make_plan(lg, j.to_leaves);
-    const uint64_t N = 1ull << lg;
-
+// Arguments shared by every pass of one transform: the direction's tables
+// (roots: omega_N powers, two-level plus the one-load table when there is
+// one; line_roots_dev: omega_4096^j), coset tables and scale of the job.
+static PassArgs transform_args(const NttJob &j, const PowTable &roots, const uint64_t *line_roots_dev) {
     PassArgs base{};
-    base.lg_n = lg;
-    base.tw_lo = rt.lo();
-    base.tw_hi = rt.hi();
-    base.tw_h = rt.h;
-    base.tw_full = rt.full;
-    base.line_roots = lr;
+    base.lg_n = j.lg;
+    base.tw_lo = roots.lo();
+    base.tw_hi = roots.hi();
+    base.tw_h = roots.h;
+    base.tw_full = roots.full;
+    base.line_roots = line_roots_dev;
     base.inverse = j.inverse ? 1u : 0u;
     base.scale = j.scale;
-    base.batches = j.batches;
+    base.batches = (uint32_t)j.batches;
     if (j.pre_coset) {
         base.pre_lo = j.pre_coset->lo();
         base.pre_hi = j.pre_coset->hi();
@@ -726,7 +718,17 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
         base.post_h = j.post_coset->h;
         base.post_full = j.post_coset->full;
     }
+    return base;
+}
 
+// Launches the passes of `plan` for job j (every transform of this file goes
+// through here): one pass, or per chunk of polynomials the column passes into
+// j.scratch and the last pass (rows, or the leaf layout with `tuned`'s
+// polynomials per block when it names one).
+static void launch_plan(const NttJob &j, const PassArgs &base, const Plan &plan, const LeavesChoice &tuned,
+                 cudaStream_t s) {
+    const uint32_t lg = j.lg;
+    const uint64_t N = 1ull << lg;
     if (plan.passes == 1) {
         PassArgs a = base;
         a.kind = 2;
@@ -818,6 +820,19 @@ void ntt_run(const NttJob &j, cudaStream_t s) {
     }
 }
 
+// One batched transform of `batches` polynomials of 2^lg elements.
+void ntt_run(const NttJob &j, cudaStream_t s) {
+    const uint32_t lg = j.lg;
+    require(lg >= 1 && lg <= 32, "transform size out of range");
+    if (j.batches == 0) return;
+    DeviceCtx &ctx = device_ctx(current_device());
+    const PowTable &rt = root_table(ctx, lg, j.inverse);
+    const uint64_t *lr = line_roots(ctx, j.inverse);
+    const LeavesChoice tuned = j.to_leaves ? leaves_choice(lg, j.batches) : LeavesChoice{};
+    const Plan plan = tuned.passes ? plan_with_passes(lg, tuned.passes) : make_plan(lg, j.to_leaves);
+    launch_plan(j, transform_args(j, rt, lr), plan, tuned, s);
+}
+
 uint64_t ntt_scratch_elems(uint32_t lg, uint64_t batches) {
     if (make_plan(lg).passes == 1) return 0;
     const uint64_t N = 1ull << lg;
@@ -861,86 +876,12 @@ namespace zk {
 
 // The transform of ntt_run, but on tables the caller supplies (no per-device
 // state is created or looked up, so nothing is allocated here): used by the
-// allocation-free LDE entry point in noalloc.cu.
+// allocation-free LDE entry point in noalloc.cu.  Same pass setup as ntt_run
+// (launch_plan), with the static plan.
 void ntt_run_on_tables(const NttJob &j, const PowTable &roots, const uint64_t *line_roots_dev, cudaStream_t s) {
-    const uint32_t lg = j.lg;
+    require(j.lg >= 1 && j.lg <= 32 && !j.to_leaves, "transform size out of range");
     if (j.batches == 0) return;
-    const Plan plan = make_plan(lg);
-    const uint64_t N = 1ull << lg;
-    PassArgs base{};
-    base.lg_n = lg;
-    base.tw_lo = roots.lo();
-    base.tw_hi = roots.hi();
-    base.tw_h = roots.h;
-    base.line_roots = line_roots_dev;
-    base.inverse = j.inverse ? 1u : 0u;
-    base.scale = j.scale;
-    base.batches = j.batches;
-    if (j.pre_coset) {
-        base.pre_lo = j.pre_coset->lo();
-        base.pre_hi = j.pre_coset->hi();
-        base.pre_h = j.pre_coset->h;
-        base.pre_full = j.pre_coset->full;
-    }
-    if (j.post_coset) {
-        base.post_lo = j.post_coset->lo();
-        base.post_hi = j.post_coset->hi();
-        base.post_h = j.post_coset->h;
-        base.post_full = j.post_coset->full;
-    }
-    if (plan.passes == 1) {
-        PassArgs a = base;
-        a.kind = 2;
-        a.l = lg;
-        a.lg_pre = 0;
-        a.lg_t = std::min<uint32_t>(ilog2_floor(kLinesElems) - lg, 6);
-        a.src = j.src;
-        a.dst = j.dst;
-        a.src_poly_stride = j.src_stride;
-        a.dst_poly_stride = j.dst_stride;
-        a.n_valid = j.n_valid;
-        launch_pass(a, (j.batches + (1ull << a.lg_t) - 1) >> a.lg_t, s, false);
-        return;
-    }
-    const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(j.batches, j.scratch_elems / N));
-    for (uint64_t b0 = 0; b0 < j.batches; b0 += chunk) {
-        const uint64_t nb = std::min<uint64_t>(chunk, j.batches - b0);
-        uint32_t lg_s = lg;
-        for (int p = 0; p < plan.passes; p++) {
-            PassArgs a = base;
-            a.l = plan.l[p];
-            a.l_first = plan.l[0];
-            a.batches = (uint32_t)nb;
-            if (p < plan.passes - 1) {
-                lg_s -= a.l;
-                a.kind = 0;
-                a.lg_s = lg_s;
-                a.lg_pre = lg - a.l - lg_s;
-                a.lg_t = std::min<uint32_t>(std::min<uint32_t>(ilog2_floor(kLinesElems) - a.l, lg_s), 5);
-                a.src = p == 0 ? j.src + b0 * j.src_stride : j.scratch;
-                a.src_poly_stride = p == 0 ? j.src_stride : N;
-                a.n_valid = p == 0 ? j.n_valid : N;
-                if (p != 0) a.pre_lo = nullptr;
-                a.dst = j.scratch;
-                a.dst_poly_stride = N;
-                a.post_lo = nullptr;
-                a.scale = 1;
-                launch_pass(a, nb << (lg - a.l - a.lg_t), s, p > 0);
-            } else {
-                a.kind = 1;
-                a.lg_s = 0;
-                a.lg_pre = lg - a.l;
-                a.lg_t = std::min<uint32_t>(std::min<uint32_t>(ilog2_floor(kLinesElems) - a.l, plan.l[0]), 5);
-                a.src = j.scratch;
-                a.src_poly_stride = N;
-                a.dst = j.dst + b0 * j.dst_stride;
-                a.dst_poly_stride = j.dst_stride;
-                a.pre_lo = nullptr;
-                a.n_valid = N;
-                launch_pass(a, nb << (a.lg_pre - a.lg_t), s, true);
-            }
-        }
-    }
+    launch_plan(j, transform_args(j, roots, line_roots_dev), make_plan(j.lg), LeavesChoice{}, s);
 }
 
 // Times every legal (passes, polynomials per block) pair of the LDE -> leaves

@@ -131,6 +131,16 @@ const PowTable &root_table(DeviceCtx &c, unsigned lg, bool inv) {
     return t;
 }
 
+namespace {
+constexpr int kGenDevices = 64;
+std::atomic<uint64_t> g_coset_gen[kGenDevices];  // 0: none installed yet
+}  // namespace
+
+uint64_t installed_coset_generator(int dev) {
+    const uint64_t g = (dev >= 0 && dev < kGenDevices) ? g_coset_gen[dev].load(std::memory_order_acquire) : 0;
+    return g ? g : GROUP_GENERATOR;
+}
+
 const PowTable &coset_table(DeviceCtx &c, unsigned lg, uint64_t gen, bool replace) {
     std::lock_guard<std::mutex> g(c.mu);
     PowTable &t = c.coset;
@@ -148,6 +158,7 @@ const PowTable &coset_table(DeviceCtx &c, unsigned lg, uint64_t gen, bool replac
         }
         t = make_pow_table(want_gen, want_bits);
     }
+    if (c.dev >= 0 && c.dev < kGenDevices) g_coset_gen[c.dev].store(t.base, std::memory_order_release);
     return t;
 }
 

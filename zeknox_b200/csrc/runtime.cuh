@@ -41,6 +41,9 @@ void note_launch();
 
 uint64_t launch_count();
 
+// Records a failure on this thread for zk_last_error() (capi.cu).
+void record_last_error(int code, const char *msg);
+
 inline void require(bool ok, const std::string &msg) {
     if (!ok) throw Error((int)cudaErrorInvalidValue, msg);
 }
@@ -104,6 +107,10 @@ const PowTable &coset_table(DeviceCtx &c, unsigned lg, uint64_t gen, bool replac
 // Powers of an arbitrary base for 2^bits exponents, built once per (base, bits)
 // and never replaced (the shifted cosets of FRI rounds use these).
 const PowTable &shift_table(DeviceCtx &c, unsigned bits, uint64_t base);
+// The coset generator the coset LDEs of device `dev` use: the one init_coset
+// installed last, GROUP_GENERATOR before that.  A plain read of a per-device
+// word (no context or table is created), for the allocation-free LDE.
+uint64_t installed_coset_generator(int dev);
 
 // Stream-ordered scratch from the device's default memory pool.
 struct Scratch {

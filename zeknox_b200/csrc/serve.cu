@@ -12,17 +12,23 @@
 // thread admits queued jobs onto free slots while their device memory fits an
 // HBM budget (reserved in the device's memory pool when the server starts, so
 // an admitted job never waits for physical memory); admitted jobs run
-// concurrently.  Jobs are split by estimated GPU time into two lanes.  Small
-// jobs are admitted shortest-first with aging (estimated time minus half the
-// time waited).  Large jobs are admitted in arrival order, one at a time (two
-// large trees sharing the GPU only delay each other), and while the oldest
-// large job waits for memory, small jobs are admitted only if they leave room
-// for it.  Jobs under 20 ms of estimated GPU time run on high-priority
-// streams, so their blocks are scheduled onto SMs ahead of those of larger
-// jobs already running.  The tree (leaves + digests + cap) of every job stays
-// resident on the device until the client releases it; the cap is also copied
-// to the host.  Completions are queued in order for zk_server_wait_any.
-// Latency (submit to completion of the cap copy) is recorded for p50 / p99.
+// concurrently.  Admission keeps every job's completion within what a FIFO
+// queue served one job at a time would give it: at submission each job gets a
+// virtual FIFO finish time F = max(now, F_prev) + est (est: the job's
+// estimated GPU time alone), and a job may start ahead of older queued jobs,
+// or beside running ones, only while the work it adds (est) fits in the
+// smallest slack (F + a tenth of that job's own est) - projected finish of
+// every job it would delay.  The
+// oldest queued job is held back the same way, so a large job is never
+// slowed past its FIFO estimate by later arrivals; small jobs fill the slack,
+// shortest first.  While the oldest job waits for memory, others are admitted
+// only if they leave room for it.  Jobs under 20 ms of estimated GPU time run
+// on high-priority streams, so their blocks are scheduled onto SMs ahead of
+// those of larger jobs already running.  The tree (leaves + digests + cap) of
+// every job stays resident on the device until the client releases it; the
+// cap is also copied to the host.  Completions are queued in order for
+// zk_server_wait_any.  Latency (submit to completion of the cap copy) is
+// recorded for p50 / p99.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -35,6 +41,7 @@
 #include <deque>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -284,20 +291,32 @@ struct ZkServer {
         uint64_t *d_scratch = nullptr;
         uint64_t *h_cap = nullptr;  // pinned copy of the cap
         int slot = -1;
-        double est_s = 0;           // estimated GPU time
+        double est_s = 0;           // estimated GPU time alone
+        double fifo_finish = 0;     // virtual FIFO finish, seconds since the server's epoch
+        double t_admit = 0;         // seconds since the epoch
+        bool seeded = false;        // coefficients generated on the device from `seed`
+        uint64_t seed = 0;
         cudaStream_t stream = nullptr;  // the stream the job ran on
-        bool big = false;
         uint64_t seq = 0;           // submission order
         int state = 0;              // 0 queued, 1 running, 2 done, 3 failed
         int err = 0;
+        std::string err_msg;        // why it failed (state 3)
     };
     int dev = 0;
     uint64_t budget = 0, in_use = 0, peak = 0;
-    double big_s = 0.2;  // jobs estimated above this many GPU seconds take the large-job lane
+    // Admission: a job's added work counts kSlackSafety times against the
+    // slack, and every job tolerates slack_frac of its own estimated GPU time
+    // beyond its FIFO finish (room for short jobs beside a long one; the
+    // long job's latency grows by at most that fraction of its service time).
+    static constexpr double kSlackSafety = 1.25;
+    double slack_frac = 0.1;
+    std::chrono::steady_clock::time_point epoch = std::chrono::steady_clock::now();
+    double vclock = 0;   // virtual FIFO finish of the last submitted job
+    uint64_t late = 0;   // completed jobs that finished after their virtual FIFO finish
     // [slot][0]: high priority, [1]: normal priority, [2]: the slot's host-to-device copies
     std::vector<std::vector<cudaStream_t>> slots;
     std::vector<bool> slot_busy;
-    int running_big = 0;
+    std::vector<uint64_t> running;     // tickets of admitted, unfinished jobs
     std::mutex mu;
     std::condition_variable cv;        // dispatcher wake-up
     std::condition_variable done_cv;   // completions
@@ -314,8 +333,16 @@ struct ZkServer {
     std::chrono::steady_clock::time_point t_first{}, t_last{};
     bool any = false;
     std::string fatal;
+    // Host-side fault injection (zk_server_inject_failure): the next
+    // inject_jobs admitted jobs fail at their inject_step-th device allocation.
+    uint32_t inject_jobs = 0, inject_step = 0;
 
     void run();
+    void fail_admitted(Job &J, const char *why);
+    double since_epoch(std::chrono::steady_clock::time_point t) const {
+        return std::chrono::duration<double>(t - epoch).count();
+    }
+    uint64_t submit(std::unique_ptr<Job> J);
 };
 
 namespace {
@@ -335,8 +362,9 @@ void CUDART_CB on_done(void *p) {
     J.t_done = std::chrono::steady_clock::now();
     J.state = 2;
     srv->slot_busy[J.slot] = false;
-    if (J.big) srv->running_big--;
+    srv->running.erase(std::find(srv->running.begin(), srv->running.end(), d->ticket));
     srv->n_running--;
+    if (srv->since_epoch(J.t_done) > J.fifo_finish + srv->slack_frac * J.est_s) srv->late++;
     srv->done_q.push_back(d->ticket);
     srv->in_use -= J.run_bytes;  // coeffs + scratch were freed on the stream before this point
     srv->latencies.push_back(std::chrono::duration<double>(J.t_done - J.t_submit).count());
@@ -365,6 +393,7 @@ void ZkServer::run() {
             if (J.bytes + J.run_bytes > budget) {
                 J.state = 3;
                 J.err = (int)cudaErrorMemoryAllocation;
+                J.err_msg = "job larger than the HBM budget";
                 done_q.push_back(*it);
                 done_cv.notify_all();
                 it = queue.erase(it);
@@ -372,33 +401,45 @@ void ZkServer::run() {
                 ++it;
             }
         }
-        // The oldest large job goes next when no other large job runs and it
-        // fits; otherwise the small job with the smallest estimated time minus
-        // half its waiting time (shortest-job-first with aging) that fits and,
-        // while that large job waits for memory, leaves room for it.
-        auto pick = queue.end(), big_head = queue.end();
-        for (auto it = queue.begin(); it != queue.end(); ++it) {
-            const Job &J = *jobs[*it];
-            if (J.big && (big_head == queue.end() || J.seq < jobs[*big_head]->seq)) big_head = it;
+        if (queue.empty()) continue;
+        // Slack admission (see the header): W is the estimated remaining work of
+        // the running jobs; a job may start when its estimate, times the safety
+        // factor, fits in the smallest slack of everything it would delay (the
+        // running jobs and the older queued ones), and it fits the budget next
+        // to the memory the oldest queued job is waiting for.  Among those the
+        // shortest goes first.
+        const double now = since_epoch(std::chrono::steady_clock::now());
+        double W = 0;
+        for (uint64_t r : running) {
+            const Job &R = *jobs[r];
+            W += std::max(0.0, R.est_s - (now - R.t_admit));
         }
+        auto deadline = [&](const Job &J) { return J.fifo_finish + slack_frac * J.est_s; };
+        double min_slack = 1e300;
+        for (uint64_t r : running) min_slack = std::min(min_slack, deadline(*jobs[r]) - (now + W));
+        std::vector<uint64_t> order(queue.begin(), queue.end());  // the queue is kept in submission order
         uint64_t reserve = 0;
-        if (big_head != queue.end() && running_big == 0) {
-            const Job &B = *jobs[*big_head];
-            if (in_use + B.bytes + B.run_bytes <= budget) pick = big_head;
-            else reserve = B.bytes + B.run_bytes;
+        {
+            const Job &H = *jobs[order.front()];
+            if (in_use + H.bytes + H.run_bytes > budget) reserve = H.bytes + H.run_bytes;
+        }
+        auto pick = queue.end();
+        double best = 1e300, cum = W;
+        for (size_t q = 0; q < order.size(); q++) {
+            const Job &J = *jobs[order[q]];
+            const uint64_t need = J.bytes + J.run_bytes + (q == 0 ? 0 : reserve);
+            if (J.est_s * kSlackSafety <= min_slack && in_use + need <= budget && J.est_s < best) {
+                best = J.est_s;
+                pick = queue.begin() + q;
+            }
+            cum += J.est_s;
+            min_slack = std::min(min_slack, deadline(J) - (now + cum));
         }
         if (pick == queue.end()) {
-            double best = 1e300;
-            const auto now = std::chrono::steady_clock::now();
-            for (auto it = queue.begin(); it != queue.end(); ++it) {
-                const Job &J = *jobs[*it];
-                if (J.big || in_use + J.bytes + J.run_bytes + reserve > budget) continue;
-                const double key = J.est_s - 0.5 * std::chrono::duration<double>(now - J.t_submit).count();
-                if (key < best) best = key, pick = it;
-            }
-        }
-        if (pick == queue.end()) {  // nothing can go until a job completes or memory is released
-            cv.wait(lk);
+            // nothing can go until a job completes, memory is released, or (jobs
+            // running past their estimate shrink the slack, ones ahead of it grow
+            // it) the projection changes: look again shortly
+            cv.wait_for(lk, std::chrono::milliseconds(2));
             continue;
         }
         const uint64_t t = *pick;
@@ -408,10 +449,16 @@ void ZkServer::run() {
         slot_busy[s] = true;
         J.slot = s;
         J.state = 1;
-        if (J.big) running_big++;
+        J.t_admit = since_epoch(std::chrono::steady_clock::now());
+        running.push_back(t);
         n_running++;
         in_use += J.bytes + J.run_bytes;
         peak = std::max(peak, in_use);
+        uint32_t fail_at = 0;  // 1-based allocation that is made to fail (0: none)
+        if (inject_jobs) {
+            inject_jobs--;
+            fail_at = inject_step;
+        }
         lk.unlock();
         try {
             // priority by size: < 20 ms of estimated GPU time high, everything else normal.  (A third,
@@ -420,34 +467,68 @@ void ZkServer::run() {
             cudaStream_t st = slots[s][J.est_s < 0.02 ? 0 : 1];
             J.stream = st;
             const Shape &sh = J.sh;
-            ZK_CUDA(cudaMallocAsync((void **)&J.d_coeffs, sh.coeff_bytes(), st));
-            ZK_CUDA(cudaMallocAsync((void **)&J.d_leaves, sh.leaf_bytes(), st));
-            if (sh.n_digests()) ZK_CUDA(cudaMallocAsync((void **)&J.d_digests, sh.digest_bytes(), st));
-            ZK_CUDA(cudaMallocAsync((void **)&J.d_cap, sh.cap_bytes(), st));
-            if (sh.scratch_bytes()) ZK_CUDA(cudaMallocAsync((void **)&J.d_scratch, sh.scratch_bytes(), st));
-            commit_from_host(ctx, sh, J.host_coeffs, J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch, st,
-                             slots[s][2]);
+            uint32_t step = 0;
+            auto alloc = [&](uint64_t **p, uint64_t bytes) {
+                if (++step == fail_at)
+                    throw Error((int)cudaErrorMemoryAllocation, "injected allocation failure");
+                ZK_CUDA(cudaMallocAsync((void **)p, bytes, st));
+            };
+            alloc(&J.d_coeffs, sh.coeff_bytes());
+            alloc(&J.d_leaves, sh.leaf_bytes());
+            if (sh.n_digests()) alloc(&J.d_digests, sh.digest_bytes());
+            alloc(&J.d_cap, sh.cap_bytes());
+            if (sh.scratch_bytes()) alloc(&J.d_scratch, sh.scratch_bytes());
+            if (J.seeded) {
+                salt_run(J.d_coeffs, sh.n() * sh.batches, J.seed, st);  // the job's input, generated in place
+                commit_on(ctx, sh, J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch, st);
+            } else {
+                commit_from_host(ctx, sh, J.host_coeffs, J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch,
+                                 st, slots[s][2]);
+            }
             ZK_CUDA(cudaMemcpyAsync(J.h_cap, J.d_cap, sh.cap_bytes(), cudaMemcpyDeviceToHost, st));
             ZK_CUDA(cudaFreeAsync(J.d_coeffs, st));
             J.d_coeffs = nullptr;
             if (J.d_scratch) ZK_CUDA(cudaFreeAsync(J.d_scratch, st));
             J.d_scratch = nullptr;
             ZK_CUDA(cudaLaunchHostFunc(st, on_done, new DoneCtx{this, t}));
-        } catch (const std::exception &e) {
+        } catch (const Error &e) {
+            J.err = e.code;
+            fail_admitted(J, e.what());
             lk.lock();
-            J.state = 3;
-            J.err = -1;
-            slot_busy[s] = false;
-            if (J.big) running_big--;
-            n_running--;
-            done_q.push_back(t);
-            in_use -= J.bytes + J.run_bytes;
-            fatal = e.what();
-            done_cv.notify_all();
+            continue;
+        } catch (const std::exception &e) {
+            J.err = -(int)cudaErrorUnknown;
+            fail_admitted(J, e.what());
+            lk.lock();
             continue;
         }
         lk.lock();
     }
+}
+
+// A job that failed after admission (an allocation or a launch threw): wait
+// for whatever of its work was already queued on its slot's streams, free the
+// allocations it made, then release its slot and its share of the budget, so
+// later jobs run as if it had never been admitted.  Called without `mu` held.
+void ZkServer::fail_admitted(Job &J, const char *why) {
+    const int s = J.slot;
+    for (cudaStream_t st : slots[s]) cudaStreamSynchronize(st);
+    for (uint64_t **p : {&J.d_coeffs, &J.d_leaves, &J.d_digests, &J.d_cap, &J.d_scratch}) {
+        if (*p) cudaFreeAsync(*p, J.stream ? J.stream : slots[s][1]);
+        *p = nullptr;
+    }
+    for (cudaStream_t st : slots[s]) cudaStreamSynchronize(st);
+    cudaGetLastError();  // the failure is reported through the job, not left for the next call
+    std::lock_guard<std::mutex> g(mu);
+    J.state = 3;
+    J.err_msg = why ? why : "job failed";
+    slot_busy[s] = false;
+    running.erase(std::find(running.begin(), running.end(), J.ticket));
+    n_running--;
+    done_q.push_back(J.ticket);
+    in_use -= J.bytes + J.run_bytes;
+    cv.notify_all();
+    done_cv.notify_all();
 }
 
 extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes, uint32_t n_slots, ZkServer **out) {
@@ -458,8 +539,9 @@ extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes,
         auto srv = std::make_unique<ZkServer>();
         srv->dev = device;
         srv->budget = hbm_budget_bytes;
-        // ZK_SERVER_BIG_JOB_S overrides the large-job threshold (seconds of estimated GPU time).
-        if (const char *e = getenv("ZK_SERVER_BIG_JOB_S")) srv->big_s = atof(e);
+        // ZK_SERVER_SLACK_FRAC overrides the tolerated delay past the FIFO estimate
+        // (a fraction of each job's own estimated GPU time; 0 = strict FIFO finish times).
+        if (const char *e = getenv("ZK_SERVER_SLACK_FRAC")) srv->slack_frac = std::max(0.0, atof(e));
         int least = 0, greatest = 0;
         ZK_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         const int levels[2] = {greatest, (greatest + least) / 2};  // high, normal
@@ -503,44 +585,79 @@ extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes,
     });
 }
 
+namespace {
+
+// GPU time of a commit alone, from its size: a fixed cost per tree level
+// (each level is a launch of a few microseconds of latency at least), the
+// permutations at ~1.0e9 per second and the LDE at ~60e9 evaluations per
+// second (B200 figures of the drop-in path; only the relative sizes matter to
+// the ordering, the absolute ones to the slack).
+double estimate_s(const Shape &sh) {
+    const double levels = (double)(sh.lg_n + sh.rate);
+    return 1.0e-4 + 1.5e-5 * levels + sh.work() / 1.0e9 + (double)sh.N() * sh.batches / 60e9;
+}
+
+std::unique_ptr<ZkServer::Job> new_job(ZkServer *srv, const Shape &sh) {
+    validate(sh);
+    {
+        // Tables are created on the caller's thread, before the job can run.
+        ZK_CUDA(cudaSetDevice(srv->dev));
+        DeviceCtx &ctx = device_ctx(srv->dev);
+        coset_table(ctx, sh.lg_n + sh.rate, GROUP_GENERATOR, false);
+        root_table(ctx, sh.lg_n + sh.rate, false);
+        line_roots(ctx, false);
+    }
+    auto J = std::make_unique<ZkServer::Job>();
+    J->sh = sh;
+    J->bytes = sh.leaf_bytes() + sh.digest_bytes() + sh.cap_bytes();
+    J->est_s = estimate_s(sh);
+    J->run_bytes = sh.coeff_bytes() + sh.scratch_bytes();
+    ZK_CUDA(cudaMallocHost((void **)&J->h_cap, sh.cap_bytes()));
+    return J;
+}
+
+}  // namespace
+
+uint64_t ZkServer::submit(std::unique_ptr<Job> J) {
+    std::lock_guard<std::mutex> g(mu);
+    require(fatal.empty(), "server failed: " + fatal);
+    J->ticket = next_ticket++;
+    J->seq = J->ticket;
+    J->t_submit = std::chrono::steady_clock::now();
+    const double t = since_epoch(J->t_submit);
+    J->fifo_finish = std::max(t, vclock) + J->est_s;
+    vclock = J->fifo_finish;
+    if (!any) {
+        t_first = J->t_submit;
+        any = true;
+    }
+    const uint64_t ticket = J->ticket;
+    queue.push_back(ticket);
+    max_queue = std::max<uint64_t>(max_queue, queue.size());
+    jobs[ticket] = std::move(J);
+    cv.notify_all();
+    return ticket;
+}
+
 extern "C" RustError zk_server_submit(ZkServer *srv, const void *host_coeffs, uint32_t lg_n, uint32_t rate_bits,
                                      uint32_t batches, uint32_t cap_height, uint32_t hash_type, uint64_t *ticket) {
     return guard([&] {
         require(srv && host_coeffs && ticket, "null argument");
-        Shape sh{lg_n, rate_bits, batches, cap_height, hash_type};
-        validate(sh);
-        {
-            // Tables are created on the caller's thread, before the job can run.
-            ZK_CUDA(cudaSetDevice(srv->dev));
-            DeviceCtx &ctx = device_ctx(srv->dev);
-            coset_table(ctx, lg_n + rate_bits, GROUP_GENERATOR, false);
-            root_table(ctx, lg_n + rate_bits, false);
-            line_roots(ctx, false);
-        }
-        auto J = std::make_unique<ZkServer::Job>();
-        J->sh = sh;
+        auto J = new_job(srv, Shape{lg_n, rate_bits, batches, cap_height, hash_type});
         J->host_coeffs = host_coeffs;
-        J->bytes = sh.leaf_bytes() + sh.digest_bytes() + sh.cap_bytes();
-        // GPU time estimate from the permutation count (about 0.8e9 Poseidon
-        // permutations per second on a B200); only the ordering matters.
-        J->est_s = sh.work() / 0.8e9;
-        J->big = J->est_s > srv->big_s;
-        J->run_bytes = sh.coeff_bytes() + sh.scratch_bytes();
-        ZK_CUDA(cudaMallocHost((void **)&J->h_cap, sh.cap_bytes()));
-        std::lock_guard<std::mutex> g(srv->mu);
-        require(srv->fatal.empty(), "server failed: " + srv->fatal);
-        J->ticket = srv->next_ticket++;
-        J->seq = J->ticket;
-        J->t_submit = std::chrono::steady_clock::now();
-        if (!srv->any) {
-            srv->t_first = J->t_submit;
-            srv->any = true;
-        }
-        *ticket = J->ticket;
-        srv->queue.push_back(J->ticket);
-        srv->max_queue = std::max<uint64_t>(srv->max_queue, srv->queue.size());
-        srv->jobs[J->ticket] = std::move(J);
-        srv->cv.notify_all();
+        *ticket = srv->submit(std::move(J));
+    });
+}
+
+extern "C" RustError zk_server_submit_seeded(ZkServer *srv, uint64_t seed, uint32_t lg_n, uint32_t rate_bits,
+                                            uint32_t batches, uint32_t cap_height, uint32_t hash_type,
+                                            uint64_t *ticket) {
+    return guard([&] {
+        require(srv && ticket, "null argument");
+        auto J = new_job(srv, Shape{lg_n, rate_bits, batches, cap_height, hash_type});
+        J->seeded = true;
+        J->seed = seed;
+        *ticket = srv->submit(std::move(J));
     });
 }
 
@@ -552,8 +669,10 @@ extern "C" RustError zk_server_wait(ZkServer *srv, uint64_t ticket, uint64_t *ho
         require(it != srv->jobs.end(), "unknown ticket");
         ZkServer::Job *J = it->second.get();
         srv->done_cv.wait(lk, [&] { return J->state >= 2 || !srv->fatal.empty(); });
-        require(J->state == 2, J->err == (int)cudaErrorMemoryAllocation ? "job larger than the HBM budget"
-                                                                          : "job failed: " + srv->fatal);
+        if (J->state == 3)
+            throw Error(J->err ? J->err : -(int)cudaErrorUnknown,
+                        J->err_msg.empty() ? std::string("job failed") : "job failed: " + J->err_msg);
+        require(J->state == 2, "job failed: " + srv->fatal);
         if (host_cap) memcpy(host_cap, J->h_cap, J->sh.cap_bytes());
         if (latency_s) *latency_s = std::chrono::duration<double>(J->t_done - J->t_submit).count();
     });
@@ -635,6 +754,16 @@ extern "C" RustError zk_server_stats(ZkServer *srv, ZkServerStats *out) {
         out->elems_per_s = span > 0 ? srv->elems_done / span : 0.0;
         out->hbm_in_use = srv->in_use;
         out->hbm_peak = srv->peak;
+        out->late = srv->late;
+    });
+}
+
+extern "C" RustError zk_server_inject_failure(ZkServer *srv, uint32_t n_jobs, uint32_t at_allocation) {
+    return guard([&] {
+        require(srv != nullptr && at_allocation >= 1, "invalid arguments");
+        std::lock_guard<std::mutex> g(srv->mu);
+        srv->inject_jobs = n_jobs;
+        srv->inject_step = at_allocation;
     });
 }
 
