@@ -907,8 +907,10 @@ def batched_section(args, zk, torch, baseline_legs: bool) -> dict:
         for j, it in zip(wave, items):
             caps_batch[j] = it[4].cap.cpu().numpy()
             it[4].cap.zero_()
-        # the same wave captured once into a CUDA graph (capture outside the timed region), replayed
+        # the same wave captured once into a CUDA graph (capture and the first replay, which maps the
+        # graph's memory, outside the timed region), replayed
         g = zk.CommitGraph(items, n_streams=args.streams)
+        g.replay()
         for it in items:
             it[4].cap.zero_()
         torch.cuda.synchronize()
@@ -1000,10 +1002,11 @@ def served_section(args, zk, torch, baseline_legs: bool) -> dict:
     plain_job(0)
     torch.cuda.synchronize()
     service, caps_plain = [], []
-    for j in range(n_jobs):
-        t0 = time.perf_counter()
-        caps_plain.append(plain_job(j))
-        service.append(time.perf_counter() - t0)
+    with ClockSampler(torch.cuda.current_device()) as clk_plain:
+        for j in range(n_jobs):
+            t0 = time.perf_counter()
+            caps_plain.append(plain_job(j))
+            service.append(time.perf_counter() - t0)
     cap_jobs_per_s = n_jobs / sum(service)
     rng = np.random.default_rng(0x5EED0055)
     arrivals = {f: np.cumsum(rng.exponential(1.0 / (f * cap_jobs_per_s), n_jobs)) for f in args.served_rates}
@@ -1013,6 +1016,7 @@ def served_section(args, zk, torch, baseline_legs: bool) -> dict:
            "jobs": n_jobs, "elems": elems, "plain_capacity_jobs_per_s": cap_jobs_per_s,
            "plain_capacity_elems_per_s": elems / sum(service), "plain_streamed_jobs": plain.streamed,
            "plain_service_s": {"p50": _pct(service, 50), "p99": _pct(service, 99), "max": max(service)},
+           "plain_service_clocks": clk_plain.summary(),
            "slots": args.streams, "budget_gb": args.budget_gb, "rates": {}}
 
     replay = {}
@@ -1051,15 +1055,16 @@ def served_section(args, zk, torch, baseline_legs: bool) -> dict:
                         errs.append(e)
 
                 th = threading.Thread(target=client)
-                th.start()
-                t0 = time.perf_counter()
-                for j, a in enumerate(arrivals[f]):
-                    now = time.perf_counter() - t0
-                    if now < a:
-                        time.sleep(a - now)
-                    lg, b, _ = jobs[j]
-                    tick[j] = srv.submit_seeded(seeds[j], lg, b, r, ch)
-                th.join()
+                with ClockSampler(torch.cuda.current_device()) as clk:
+                    th.start()
+                    t0 = time.perf_counter()
+                    for j, a in enumerate(arrivals[f]):
+                        now = time.perf_counter() - t0
+                        if now < a:
+                            time.sleep(a - now)
+                        lg, b, _ = jobs[j]
+                        tick[j] = srv.submit_seeded(seeds[j], lg, b, r, ch)
+                    th.join()
                 if errs:
                     raise errs[0]
                 span = time.perf_counter() - t0 - arrivals[f][0]
@@ -1068,16 +1073,16 @@ def served_section(args, zk, torch, baseline_legs: bool) -> dict:
             all_caps_ok &= ok
             lats = [lat_s[tick[j]] for j in range(n_jobs)]
             runs.append({"p50_s": _pct(lats, 50), "p99_s": _pct(lats, 99), "elems_per_s": elems / span,
-                         "late_jobs": st["late"], "max_queue": st["max_queue"],
-                         "hbm_peak_gb": st["hbm_peak"] / 2**30})
+                         "started_ahead": st["ahead"], "max_queue": st["max_queue"],
+                         "hbm_peak_gb": st["hbm_peak"] / 2**30, "clocks": clk.summary()})
         med = lambda k: float(np.median([x[k] for x in runs]))  # noqa: E731
         entry = {
             "arrival_jobs_per_s": f * cap_jobs_per_s,
             "plain": {"p50_s": _pct(lat_p, 50), "p99_s": _pct(lat_p, 99), "elems_per_s": elems / span_p,
                       "how": "real-time replay" if f in replay else "FIFO over measured service times"},
             "served": {"p50_s": med("p50_s"), "p99_s": med("p99_s"), "elems_per_s": med("elems_per_s"),
-                       "late_jobs": int(med("late_jobs")), "max_queue": int(med("max_queue")),
-                       "hbm_peak_gb": med("hbm_peak_gb")},
+                       "started_ahead": int(med("started_ahead")), "max_queue": int(med("max_queue")),
+                       "hbm_peak_gb": med("hbm_peak_gb"), "clocks": runs[len(runs) // 2]["clocks"]},
         }
         if len(runs) > 1:
             entry["served"]["runs"] = runs

@@ -241,10 +241,11 @@ ZK_EXTERN RustError zk_autotune_reset(void);
  * caller until the job completes), admitted onto n_slots concurrent streams
  * while leaves + digests + cap of resident trees plus coefficients + scratch of
  * running jobs fit hbm_budget_bytes, and keep their tree on the device until
- * released.  Admission keeps each job within the completion time a FIFO queue
- * served one job at a time would give it (estimated from job sizes), plus a
- * tenth of its own estimated GPU time; later, shorter jobs run ahead of or
- * beside earlier ones only inside that slack.
+ * released.  Admission is first in, first out, except that a later, shorter
+ * job may start ahead of or beside earlier ones when its estimated GPU time
+ * fits in each of their delay budgets (a twentieth of each one's own
+ * estimated GPU time, from job sizes; ZK_SERVER_BUDGET_FRAC overrides the
+ * fraction), which it then uses up.
  * zk_server_wait blocks until the cap is on the host.
  * zk_server_wait_any returns, in completion order, each job that has finished
  * (or failed) since the last call, once; *ticket = 0 when nothing is pending or
@@ -256,7 +257,7 @@ typedef struct {
     double p50_s, p99_s, max_s; /* submit -> cap on the host */
     double elems, elems_per_s;  /* committed LDE evaluations; first submit -> last completion */
     uint64_t hbm_in_use, hbm_peak;
-    uint64_t late; /* completed jobs that finished after their estimated FIFO completion plus slack */
+    uint64_t ahead; /* jobs started ahead of an older queued job or beside a running one */
 } ZkServerStats;
 ZK_EXTERN RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes, uint32_t n_slots, ZkServer **out);
 ZK_EXTERN RustError zk_server_submit(ZkServer *srv, const void *host_coeffs, uint32_t lg_n, uint32_t rate_bits,

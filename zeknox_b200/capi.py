@@ -79,7 +79,7 @@ class ZkServerStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_uint64), ("queued", ctypes.c_uint64), ("max_queue", ctypes.c_uint64),
                 ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("max_s", ctypes.c_double),
                 ("elems", ctypes.c_double), ("elems_per_s", ctypes.c_double), ("hbm_in_use", ctypes.c_uint64),
-                ("hbm_peak", ctypes.c_uint64), ("late", ctypes.c_uint64)]
+                ("hbm_peak", ctypes.c_uint64), ("ahead", ctypes.c_uint64)]
 
 
 assert ctypes.sizeof(NTTConfig) == 24 and ctypes.sizeof(TransposeConfig) == 8

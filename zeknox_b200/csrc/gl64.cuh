@@ -137,39 +137,6 @@ __device__ __forceinline__ uint64_t gl_canon(uint64_t x) { return x >= ZK_P ? x 
 // ---------------------------------------------------------------------------
 namespace zk {
 
-// x + k (2^32 - 1) mod 2^64 for k in {0, 1}: one multiply-add (the fold of a
-// carry out of 2^64, 2^64 = 2^32 - 1 mod p).
-__device__ __forceinline__ uint64_t pr_fold(uint32_t k, uint64_t x) {
-    uint64_t r;
-    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(r) : "r"(k), "r"(0xffffffffu), "l"(x));
-    return r;
-}
-
-#if ZK_HASH_MAD_REDUCE
-// (h1, h0, l1, l0) 128-bit -> u64 congruent mod p:
-//   x = (l1:l0) - h1 + h0 * (2^32 - 1).
-// The subtraction takes 2^32 - 1 off on a borrow (the low word minus
-// 0xffffffff, a borrow from the high word exactly when that does not wrap);
-// h0 (2^32 - 1) is added by a mad.lo / madc.hi pair and its carry out of 2^64
-// folded once more by a multiply-add (it cannot carry again).
-__device__ __forceinline__ uint64_t pr_reduce128(uint32_t l0, uint32_t l1, uint32_t h0, uint32_t h1) {
-    uint32_t r0, r1, k;
-    asm("{\n\t"
-        ".reg .u32 b;\n\t"
-        "sub.cc.u32 %0, %3, %6;\n\t"
-        "subc.cc.u32 %1, %4, 0;\n\t"
-        "subc.u32 b, 0, 0;\n\t"
-        "sub.cc.u32 %0, %0, b;\n\t"
-        "subc.u32 %1, %1, 0;\n\t"
-        "mad.lo.cc.u32 %0, %5, %7, %0;\n\t"
-        "madc.hi.cc.u32 %1, %5, %7, %1;\n\t"
-        "addc.u32 %2, 0, 0;\n\t"
-        "}"
-        : "=r"(r0), "=r"(r1), "=r"(k)
-        : "r"(l0), "r"(l1), "r"(h0), "r"(h1), "r"(0xffffffffu));
-    return pr_fold(k, ((uint64_t)r1 << 32) | r0);
-}
-#else
 // (h1, h0, l1, l0) 128-bit -> u64 congruent mod p:
 //   x = (l1:l0) - h1 + h0 * (2^32 - 1).
 __device__ __forceinline__ uint64_t pr_reduce128(uint32_t l0, uint32_t l1, uint32_t h0, uint32_t h1) {
@@ -194,7 +161,6 @@ __device__ __forceinline__ uint64_t pr_reduce128(uint32_t l0, uint32_t l1, uint3
         : "r"(l0), "r"(l1), "r"(h0), "r"(h1));
     return ((uint64_t)r1 << 32) | r0;
 }
-#endif
 
 // a * b for any u64 a, b; result partially reduced.  The 128-bit product
 // comes from the 32-bit multiply-add chain of mul_wide (cheaper here than
@@ -237,47 +203,6 @@ __device__ __forceinline__ uint64_t pr_pow7(uint64_t x) {
     return pr_mul(x3, x4);
 }
 
-#if ZK_HASH_MAD_SPLIT
-// al + ah * 2^32 + c for any al, c < 2^64 and ah < 2^64 - 2^33; partially
-// reduced.  ah 2^32 = lo32(ah) 2^32 + hi32(ah) 2^64: the low part goes into
-// the high word, hi32(ah) plus the carries (k < 2^32) times 2^64 = 2^32 - 1
-// by a mad.lo / madc.hi pair, and that carry is folded once more.
-__device__ __forceinline__ uint64_t pr_reduce_split(uint64_t al, uint64_t ah, uint64_t c) {
-    uint32_t r0, r1, j;
-    asm("{\n\t"
-        ".reg .u32 k;\n\t"
-        "add.cc.u32  %0, %3, %7;\n\t"
-        "addc.cc.u32 %1, %4, %8;\n\t"
-        "addc.u32    k, 0, 0;\n\t"
-        "add.cc.u32  %1, %1, %5;\n\t"
-        "addc.u32    k, k, %6;\n\t"
-        "mad.lo.cc.u32 %0, k, %9, %0;\n\t"
-        "madc.hi.cc.u32 %1, k, %9, %1;\n\t"
-        "addc.u32    %2, 0, 0;\n\t"
-        "}"
-        : "=r"(r0), "=r"(r1), "=r"(j)
-        : "r"((uint32_t)al), "r"((uint32_t)(al >> 32)), "r"((uint32_t)ah), "r"((uint32_t)(ah >> 32)),
-          "r"((uint32_t)c), "r"((uint32_t)(c >> 32)), "r"(0xffffffffu));
-    return pr_fold(j, ((uint64_t)r1 << 32) | r0);
-}
-
-// al + ah * 2^32 for al < 2^64 and ah < 2^64 - 2^33; partially reduced.
-__device__ __forceinline__ uint64_t pr_reduce_split_nc(uint64_t al, uint64_t ah) {
-    uint32_t r0 = (uint32_t)al, r1, j;
-    asm("{\n\t"
-        ".reg .u32 k;\n\t"
-        "add.cc.u32  %1, %4, %5;\n\t"
-        "addc.u32    k, %6, 0;\n\t"
-        "mad.lo.cc.u32 %0, k, %7, %0;\n\t"
-        "madc.hi.cc.u32 %1, k, %7, %1;\n\t"
-        "addc.u32    %2, 0, 0;\n\t"
-        "}"
-        : "+r"(r0), "=r"(r1), "=r"(j)
-        : "r"((uint32_t)al), "r"((uint32_t)(al >> 32)), "r"((uint32_t)ah), "r"((uint32_t)(ah >> 32)),
-          "r"(0xffffffffu));
-    return pr_fold(j, ((uint64_t)r1 << 32) | r0);
-}
-#else
 // al + ah * 2^32 + c for any al, c < 2^64 and ah < 2^64 - 2^33; partially
 // reduced.
 __device__ __forceinline__ uint64_t pr_reduce_split(uint64_t al, uint64_t ah, uint64_t c) {
@@ -324,6 +249,5 @@ __device__ __forceinline__ uint64_t pr_reduce_split_nc(uint64_t al, uint64_t ah)
         : "r"((uint32_t)al), "r"((uint32_t)(al >> 32)), "r"((uint32_t)ah), "r"((uint32_t)(ah >> 32)));
     return ((uint64_t)r1 << 32) | r0;
 }
-#endif
 
 }  // namespace zk

@@ -12,16 +12,18 @@
 // thread admits queued jobs onto free slots while their device memory fits an
 // HBM budget (reserved in the device's memory pool when the server starts, so
 // an admitted job never waits for physical memory); admitted jobs run
-// concurrently.  Admission keeps every job's completion within what a FIFO
-// queue served one job at a time would give it: at submission each job gets a
-// virtual FIFO finish time F = max(now, F_prev) + est (est: the job's
-// estimated GPU time alone), and a job may start ahead of older queued jobs,
-// or beside running ones, only while the work it adds (est) fits in the
-// smallest slack (F + a tenth of that job's own est) - projected finish of
-// every job it would delay.  The
-// oldest queued job is held back the same way, so a large job is never
-// slowed past its FIFO estimate by later arrivals; small jobs fill the slack,
-// shortest first.  While the oldest job waits for memory, others are admitted
+// concurrently.  Admission is first in, first out, with one exception that
+// is bounded per job: every job carries a delay budget, a fraction of its own
+// estimated GPU time alone (est, from its size).  A job may start ahead of
+// older queued jobs, or beside running ones, only if its est fits in the
+// remaining budget of every one of those jobs, and starting it charges its
+// est to each of them.  So no job is delayed, by jobs that arrived after it,
+// by more than its budget (a long job's latency grows by at most that
+// fraction of its own service time), while short jobs start at once beside
+// long ones instead of queueing behind them; among the jobs that may start,
+// the shortest goes first.  Only relative sizes enter: estimates that are
+// off by a common factor change nothing.  While the oldest job waits for
+// memory, others are admitted
 // only if they leave room for it.  Jobs under 20 ms of estimated GPU time run
 // on high-priority streams, so their blocks are scheduled onto SMs ahead of
 // those of larger jobs already running.  The tree (leaves + digests + cap) of
@@ -292,8 +294,7 @@ struct ZkServer {
         uint64_t *h_cap = nullptr;  // pinned copy of the cap
         int slot = -1;
         double est_s = 0;           // estimated GPU time alone
-        double fifo_finish = 0;     // virtual FIFO finish, seconds since the server's epoch
-        double t_admit = 0;         // seconds since the epoch
+        double budget_s = 0;        // delay it may still take from later jobs started ahead of or beside it
         bool seeded = false;        // coefficients generated on the device from `seed`
         uint64_t seed = 0;
         cudaStream_t stream = nullptr;  // the stream the job ran on
@@ -304,15 +305,9 @@ struct ZkServer {
     };
     int dev = 0;
     uint64_t budget = 0, in_use = 0, peak = 0;
-    // Admission: a job's added work counts kSlackSafety times against the
-    // slack, and every job tolerates slack_frac of its own estimated GPU time
-    // beyond its FIFO finish (room for short jobs beside a long one; the
-    // long job's latency grows by at most that fraction of its service time).
-    static constexpr double kSlackSafety = 1.25;
-    double slack_frac = 0.1;
-    std::chrono::steady_clock::time_point epoch = std::chrono::steady_clock::now();
-    double vclock = 0;   // virtual FIFO finish of the last submitted job
-    uint64_t late = 0;   // completed jobs that finished after their virtual FIFO finish
+    // Every job's delay budget: this fraction of its own estimated GPU time.
+    double budget_frac = 0.05;
+    uint64_t ahead = 0;  // jobs started ahead of an older queued job or beside a running one
     // [slot][0]: high priority, [1]: normal priority, [2]: the slot's host-to-device copies
     std::vector<std::vector<cudaStream_t>> slots;
     std::vector<bool> slot_busy;
@@ -339,9 +334,6 @@ struct ZkServer {
 
     void run();
     void fail_admitted(Job &J, const char *why);
-    double since_epoch(std::chrono::steady_clock::time_point t) const {
-        return std::chrono::duration<double>(t - epoch).count();
-    }
     uint64_t submit(std::unique_ptr<Job> J);
 };
 
@@ -364,7 +356,6 @@ void CUDART_CB on_done(void *p) {
     srv->slot_busy[J.slot] = false;
     srv->running.erase(std::find(srv->running.begin(), srv->running.end(), d->ticket));
     srv->n_running--;
-    if (srv->since_epoch(J.t_done) > J.fifo_finish + srv->slack_frac * J.est_s) srv->late++;
     srv->done_q.push_back(d->ticket);
     srv->in_use -= J.run_bytes;  // coeffs + scratch were freed on the stream before this point
     srv->latencies.push_back(std::chrono::duration<double>(J.t_done - J.t_submit).count());
@@ -402,45 +393,42 @@ void ZkServer::run() {
             }
         }
         if (queue.empty()) continue;
-        // Slack admission (see the header): W is the estimated remaining work of
-        // the running jobs; a job may start when its estimate, times the safety
-        // factor, fits in the smallest slack of everything it would delay (the
-        // running jobs and the older queued ones), and it fits the budget next
-        // to the memory the oldest queued job is waiting for.  Among those the
-        // shortest goes first.
-        const double now = since_epoch(std::chrono::steady_clock::now());
-        double W = 0;
-        for (uint64_t r : running) {
-            const Job &R = *jobs[r];
-            W += std::max(0.0, R.est_s - (now - R.t_admit));
-        }
-        auto deadline = [&](const Job &J) { return J.fifo_finish + slack_frac * J.est_s; };
-        double min_slack = 1e300;
-        for (uint64_t r : running) min_slack = std::min(min_slack, deadline(*jobs[r]) - (now + W));
+        // Budget admission (see the header): the candidate at queue position q
+        // would delay the running jobs and the queued jobs before it; it may
+        // start if its estimate fits in each of their budgets (the oldest job,
+        // with nothing running, always may), and if it fits the HBM budget
+        // next to the memory the oldest queued job is waiting for.  Among
+        // those the shortest goes first.
         std::vector<uint64_t> order(queue.begin(), queue.end());  // the queue is kept in submission order
         uint64_t reserve = 0;
         {
             const Job &H = *jobs[order.front()];
             if (in_use + H.bytes + H.run_bytes > budget) reserve = H.bytes + H.run_bytes;
         }
+        double room = 1e300;  // smallest budget among the jobs a candidate would delay
+        for (uint64_t r : running) room = std::min(room, jobs[r]->budget_s);
         auto pick = queue.end();
-        double best = 1e300, cum = W;
+        size_t pick_q = 0;
+        double best = 1e300;
         for (size_t q = 0; q < order.size(); q++) {
             const Job &J = *jobs[order[q]];
             const uint64_t need = J.bytes + J.run_bytes + (q == 0 ? 0 : reserve);
-            if (J.est_s * kSlackSafety <= min_slack && in_use + need <= budget && J.est_s < best) {
+            if (J.est_s <= room && in_use + need <= budget && J.est_s < best) {
                 best = J.est_s;
                 pick = queue.begin() + q;
+                pick_q = q;
             }
-            cum += J.est_s;
-            min_slack = std::min(min_slack, deadline(J) - (now + cum));
+            room = std::min(room, J.budget_s);
         }
-        if (pick == queue.end()) {
-            // nothing can go until a job completes, memory is released, or (jobs
-            // running past their estimate shrink the slack, ones ahead of it grow
-            // it) the projection changes: look again shortly
-            cv.wait_for(lk, std::chrono::milliseconds(2));
+        if (pick == queue.end()) {  // nothing can go until a job completes or memory is released
+            cv.wait(lk);
             continue;
+        }
+        {
+            const Job &P = *jobs[*pick];
+            if (pick_q > 0 || !running.empty()) ahead++;
+            for (uint64_t r : running) jobs[r]->budget_s -= P.est_s;
+            for (size_t q = 0; q < pick_q; q++) jobs[order[q]]->budget_s -= P.est_s;
         }
         const uint64_t t = *pick;
         queue.erase(pick);
@@ -449,7 +437,6 @@ void ZkServer::run() {
         slot_busy[s] = true;
         J.slot = s;
         J.state = 1;
-        J.t_admit = since_epoch(std::chrono::steady_clock::now());
         running.push_back(t);
         n_running++;
         in_use += J.bytes + J.run_bytes;
@@ -539,9 +526,9 @@ extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes,
         auto srv = std::make_unique<ZkServer>();
         srv->dev = device;
         srv->budget = hbm_budget_bytes;
-        // ZK_SERVER_SLACK_FRAC overrides the tolerated delay past the FIFO estimate
-        // (a fraction of each job's own estimated GPU time; 0 = strict FIFO finish times).
-        if (const char *e = getenv("ZK_SERVER_SLACK_FRAC")) srv->slack_frac = std::max(0.0, atof(e));
+        // ZK_SERVER_BUDGET_FRAC overrides the delay budget (a fraction of each job's own
+        // estimated GPU time; 0 = first in, first out, one job at a time).
+        if (const char *e = getenv("ZK_SERVER_BUDGET_FRAC")) srv->budget_frac = std::max(0.0, atof(e));
         int least = 0, greatest = 0;
         ZK_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         const int levels[2] = {greatest, (greatest + least) / 2};  // high, normal
@@ -590,8 +577,7 @@ namespace {
 // GPU time of a commit alone, from its size: a fixed cost per tree level
 // (each level is a launch of a few microseconds of latency at least), the
 // permutations at ~1.0e9 per second and the LDE at ~60e9 evaluations per
-// second (B200 figures of the drop-in path; only the relative sizes matter to
-// the ordering, the absolute ones to the slack).
+// second (B200 figures of the drop-in path; only the relative sizes matter).
 double estimate_s(const Shape &sh) {
     const double levels = (double)(sh.lg_n + sh.rate);
     return 1.0e-4 + 1.5e-5 * levels + sh.work() / 1.0e9 + (double)sh.N() * sh.batches / 60e9;
@@ -624,9 +610,7 @@ uint64_t ZkServer::submit(std::unique_ptr<Job> J) {
     J->ticket = next_ticket++;
     J->seq = J->ticket;
     J->t_submit = std::chrono::steady_clock::now();
-    const double t = since_epoch(J->t_submit);
-    J->fifo_finish = std::max(t, vclock) + J->est_s;
-    vclock = J->fifo_finish;
+    J->budget_s = budget_frac * J->est_s;
     if (!any) {
         t_first = J->t_submit;
         any = true;
@@ -754,7 +738,7 @@ extern "C" RustError zk_server_stats(ZkServer *srv, ZkServerStats *out) {
         out->elems_per_s = span > 0 ? srv->elems_done / span : 0.0;
         out->hbm_in_use = srv->in_use;
         out->hbm_peak = srv->peak;
-        out->late = srv->late;
+        out->ahead = srv->ahead;
     });
 }
 
