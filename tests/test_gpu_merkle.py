@@ -106,7 +106,9 @@ def test_vs_reference_cpu_fixtures(zk, oracle, golden):
                                      # hand-built 4-leaf trees of native/tests/tests.cu:338-375; short
                                      # leaves (no permutation) on the small-tree kernels; cap == leaves
                                      (4096, 7, 1), (4, 7, 0), (4, 7, 1), (2, 9, 0), (8192, 4, 2),
-                                     (8192, 1, 0), (1 << 13, 135, 13)])
+                                     (8192, 1, 0), (1 << 13, 135, 13),
+                                     # one thread per leaf with 128 leaves per subtree, and short leaves
+                                     (1 << 15, 9, 8), (1 << 15, 4, 6)])
 def test_vs_oracle(zk, oracle, ht, nl, ls, ch):
     leaves = oracle.field_elems(ht * 1000 + nl + ls, nl * ls)
     d, c = gpu_tree(zk, leaves, ls, ch, ht)

@@ -503,7 +503,7 @@ void lde_leaves_device(DeviceCtx &ctx, uint64_t *d_leaves, const uint64_t *d_in,
     j.lg = lg;
     j.pre_coset = coset ? coset : &coset_table(ctx, lg, GROUP_GENERATOR, false);
     j.to_leaves = true;
-    j.scratch_elems = ntt_scratch_elems(lg, batches);
+    j.scratch_elems = ntt_leaves_scratch_elems(lg, batches);
     Scratch scr(j.scratch_elems * sizeof(uint64_t), s);
     j.scratch = scr.as<uint64_t>();
     ntt_run(j, s);

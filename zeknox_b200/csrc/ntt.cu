@@ -633,6 +633,8 @@ static void launch_plan(const NttJob &j, const PassArgs &base, const Plan &plan,
                 a.lg_pre = lg - a.l;
                 a.lg_t = a.l <= 9 ? 3 : 12 - std::min<uint32_t>(a.l, 12);
                 if (tuned.passes && leaves_fits(a.l, tuned.lg_t)) a.lg_t = tuned.lg_t;
+                // no wider than the chunk (the smallest power of two >= its polynomials)
+                while (a.lg_t > 0 && (1ull << (a.lg_t - 1)) >= nb) a.lg_t--;
                 a.src = scr;
                 a.src_poly_stride = N;
                 a.dst = j.dst + b0;
@@ -682,6 +684,19 @@ uint64_t ntt_scratch_elems(uint32_t lg, uint64_t batches) {
     // last wave idle).  Always at least one polynomial.
     const uint64_t cap = (512ull << 20) / sizeof(uint64_t);
     return std::max<uint64_t>(N, std::min<uint64_t>(batches * N, cap / N * N));
+}
+
+// The leaves pass puts up to 8 polynomials in a block (8-word runs in every
+// leaf row), so the LDE -> leaves stage takes chunks of at least 8
+// polynomials when the batch has them, beyond the 512 MiB of
+// ntt_scratch_elems where need be (2 GiB for 2^25-point transforms).  With 2
+// polynomials per chunk (2^25 points), six of every eight block lines idled
+// and each leaf row got 16-byte runs: 120 x 2^22 -> 2^25 took 240 ms against
+// 141 ms for the LDE rows plus the transpose.
+uint64_t ntt_leaves_scratch_elems(uint32_t lg, uint64_t batches) {
+    const uint64_t base = ntt_scratch_elems(lg, batches);
+    if (!base) return 0;
+    return std::max<uint64_t>(base, std::min<uint64_t>(batches, 8) << lg);
 }
 
 void transpose_rev_run(uint64_t *out, const uint64_t *in, uint32_t lg_n, uint32_t batches, cudaStream_t s) {
@@ -742,7 +757,7 @@ int ntt_autotune_leaves(uint32_t lg_n, uint32_t rate_bits, uint64_t batches, cud
     // a representative batch: the class's own size, capped at ~1 GiB of leaves
     const uint64_t bt = std::max<uint64_t>(1, std::min<uint64_t>(batches, (1ull << 27) / N));
     Scratch in(bt * n * sizeof(uint64_t), s), out(bt * N * sizeof(uint64_t), s);
-    const uint64_t scr_elems = ntt_scratch_elems(lg, bt);
+    const uint64_t scr_elems = ntt_leaves_scratch_elems(lg, bt);
     Scratch scr(scr_elems * sizeof(uint64_t), s);
     ZK_CUDA(cudaMemsetAsync(in.p, 0, bt * n * sizeof(uint64_t), s));
     NttJob j;

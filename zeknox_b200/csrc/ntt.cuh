@@ -38,6 +38,8 @@ struct NttJob {
 
 void ntt_run(const NttJob &job, cudaStream_t s);
 uint64_t ntt_scratch_elems(uint32_t lg, uint64_t batches);
+// Scratch of the LDE -> leaves stage (to_leaves): chunks of at least 8 polynomials.
+uint64_t ntt_leaves_scratch_elems(uint32_t lg, uint64_t batches);
 void transpose_rev_run(uint64_t *out, const uint64_t *in, uint32_t lg_n, uint32_t batches, cudaStream_t s);
 void salt_run(uint64_t *out, uint64_t count, uint64_t seed, cudaStream_t s);
 // Autotuning of the LDE -> leaves stage per (size, batch-size class); see ntt.cu.

@@ -87,7 +87,7 @@ struct Shape {
     uint64_t leaf_bytes() const { return N() * batches * 8; }
     uint64_t digest_bytes() const { return n_digests() * 32; }
     uint64_t cap_bytes() const { return n_caps() * 32; }
-    uint64_t scratch_bytes() const { return ntt_scratch_elems(lg_n + rate, batches) * 8; }
+    uint64_t scratch_bytes() const { return ntt_leaves_scratch_elems(lg_n + rate, batches) * 8; }
 };
 
 void validate(const Shape &s) {
@@ -128,7 +128,7 @@ void lde_leaves_slice(DeviceCtx &ctx, const Shape &sh, const uint64_t *coeffs, u
     j.pre_coset = &coset_table(ctx, lg, GROUP_GENERATOR, false);
     j.to_leaves = true;
     j.scratch = scratch;
-    j.scratch_elems = ntt_scratch_elems(lg, nb);
+    j.scratch_elems = ntt_leaves_scratch_elems(lg, nb);
     ntt_run(j, st);
 }
 
@@ -291,7 +291,7 @@ struct ZkServer {
         uint64_t run_bytes = 0;     // extra bytes held while running (coeffs + scratch)
         uint64_t *d_coeffs = nullptr, *d_leaves = nullptr, *d_digests = nullptr, *d_cap = nullptr;
         uint64_t *d_scratch = nullptr;
-        uint64_t *h_cap = nullptr;  // pinned copy of the cap
+        std::vector<uint64_t> cap;  // the cap on the host, filled when the job completes
         int slot = -1;
         double est_s = 0;           // estimated GPU time alone
         double budget_s = 0;        // delay it may still take from later jobs started ahead of or beside it
@@ -310,6 +310,12 @@ struct ZkServer {
     uint64_t ahead = 0;  // jobs started ahead of an older queued job or beside a running one
     // [slot][0]: high priority, [1]: normal priority, [2]: the slot's host-to-device copies
     std::vector<std::vector<cudaStream_t>> slots;
+    // Per slot, pinned staging for the cap's device-to-host copy (grown by the
+    // dispatcher when a larger cap comes along; the completion callback copies
+    // it into the job), so that no job allocates or frees pinned memory: both
+    // can synchronise with the device.
+    std::vector<uint64_t *> slot_cap;
+    std::vector<uint64_t> slot_cap_bytes;
     std::vector<bool> slot_busy;
     std::vector<uint64_t> running;     // tickets of admitted, unfinished jobs
     std::mutex mu;
@@ -352,6 +358,7 @@ void CUDART_CB on_done(void *p) {
     if (it == srv->jobs.end()) return;
     ZkServer::Job &J = *it->second;
     J.t_done = std::chrono::steady_clock::now();
+    J.cap.assign(srv->slot_cap[J.slot], srv->slot_cap[J.slot] + J.sh.cap_bytes() / sizeof(uint64_t));
     J.state = 2;
     srv->slot_busy[J.slot] = false;
     srv->running.erase(std::find(srv->running.begin(), srv->running.end(), d->ticket));
@@ -454,6 +461,17 @@ void ZkServer::run() {
             cudaStream_t st = slots[s][J.est_s < 0.02 ? 0 : 1];
             J.stream = st;
             const Shape &sh = J.sh;
+            if (slot_cap_bytes[s] < sh.cap_bytes()) {
+                // Rare (a larger cap than this slot has staged so far), and done
+                // without the lock: pinned allocation may synchronise with the
+                // device, whose completion callbacks take the lock.  The slot is
+                // this job's, and its previous job's callback has run.
+                if (slot_cap[s]) cudaFreeHost(slot_cap[s]);
+                slot_cap[s] = nullptr;
+                slot_cap_bytes[s] = 0;
+                ZK_CUDA(cudaMallocHost((void **)&slot_cap[s], sh.cap_bytes()));
+                slot_cap_bytes[s] = sh.cap_bytes();
+            }
             uint32_t step = 0;
             auto alloc = [&](uint64_t **p, uint64_t bytes) {
                 if (++step == fail_at)
@@ -472,7 +490,7 @@ void ZkServer::run() {
                 commit_from_host(ctx, sh, J.host_coeffs, J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch,
                                  st, slots[s][2]);
             }
-            ZK_CUDA(cudaMemcpyAsync(J.h_cap, J.d_cap, sh.cap_bytes(), cudaMemcpyDeviceToHost, st));
+            ZK_CUDA(cudaMemcpyAsync(slot_cap[s], J.d_cap, sh.cap_bytes(), cudaMemcpyDeviceToHost, st));
             ZK_CUDA(cudaFreeAsync(J.d_coeffs, st));
             J.d_coeffs = nullptr;
             if (J.d_scratch) ZK_CUDA(cudaFreeAsync(J.d_scratch, st));
@@ -544,6 +562,10 @@ extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes,
             per.push_back(cs);
             srv->slots.push_back(per);
             srv->slot_busy.push_back(false);
+            uint64_t *staging = nullptr;
+            ZK_CUDA(cudaMallocHost((void **)&staging, 64 << 10));  // caps of up to 2^11 digests
+            srv->slot_cap.push_back(staging);
+            srv->slot_cap_bytes.push_back(64 << 10);
         }
         // Reserve the budget in the pool (which keeps freed memory: its release
         // threshold is unlimited), so admitted jobs are served from mapped
@@ -598,7 +620,6 @@ std::unique_ptr<ZkServer::Job> new_job(ZkServer *srv, const Shape &sh) {
     J->bytes = sh.leaf_bytes() + sh.digest_bytes() + sh.cap_bytes();
     J->est_s = estimate_s(sh);
     J->run_bytes = sh.coeff_bytes() + sh.scratch_bytes();
-    ZK_CUDA(cudaMallocHost((void **)&J->h_cap, sh.cap_bytes()));
     return J;
 }
 
@@ -657,7 +678,7 @@ extern "C" RustError zk_server_wait(ZkServer *srv, uint64_t ticket, uint64_t *ho
             throw Error(J->err ? J->err : -(int)cudaErrorUnknown,
                         J->err_msg.empty() ? std::string("job failed") : "job failed: " + J->err_msg);
         require(J->state == 2, "job failed: " + srv->fatal);
-        if (host_cap) memcpy(host_cap, J->h_cap, J->sh.cap_bytes());
+        if (host_cap) memcpy(host_cap, J->cap.data(), J->sh.cap_bytes());
         if (latency_s) *latency_s = std::chrono::duration<double>(J->t_done - J->t_submit).count();
     });
 }
@@ -715,7 +736,6 @@ extern "C" RustError zk_server_release(ZkServer *srv, uint64_t ticket) {
             srv->in_use -= J->bytes;
             srv->cv.notify_all();
         }
-        cudaFreeHost(J->h_cap);
     });
 }
 
@@ -767,10 +787,11 @@ extern "C" RustError zk_server_destroy(ZkServer *srv) {
             auto &J = *kv.second;
             for (uint64_t *p : {J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch})
                 if (p) cudaFree(p);
-            if (J.h_cap) cudaFreeHost(J.h_cap);
         }
         for (auto &per : srv->slots)
             for (cudaStream_t st : per) cudaStreamDestroy(st);
+        for (uint64_t *p : srv->slot_cap)
+            if (p) cudaFreeHost(p);
         // Hand the reserved budget back to the device.
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, srv->dev) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
