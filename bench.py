@@ -978,7 +978,9 @@ def served_section(args, zk, torch, baseline_legs: bool) -> dict:
     plain: the drop-in per-job path, one job at a time in arrival order (FIFO).  Each job's service time is
     measured once, back to back in arrival order; the FIFO latencies at each rate follow from those times
     and the arrival times (start = max(arrival, previous end)), or, with --served-replay, from a real-time
-    replay of the queue.  served: zk_server (120 GB budget, 4 slots), real time, seeded submissions."""
+    replay of the queue.  served: zk_server (120 GB budget, 4 slots), real time, seeded submissions.
+    --served-repeats R repeats both arms (service pass and served runs) on the same arrival schedule and
+    reports the medians and every run."""
     n_jobs = args.served_jobs
     ch, r = 4, 3
     jobs = _jobs(0x5EED0005, 10000, 12, 22, 8, 300, [3])[:n_jobs]
@@ -990,112 +992,138 @@ def served_section(args, zk, torch, baseline_legs: bool) -> dict:
     zk.init_coset(0, max(lg for lg, _, _ in jobs) + r, 7)
     for lg in sorted({lg + r for lg, _, _ in jobs}):
         zk.init_twiddle_factors(0, lg)
-    dev_in = torch.empty(mx_in, dtype=torch.uint64, device="cuda")
-    # the LDE matrix of a job up to 60 GB; larger ones stream (leaves up to 80.5 GB beside it)
-    plain = DropIn(torch, zk.capi.LIB, zk.capi.check, mx_in, mx, mx_n, (60 << 30) // 8)
+    # the LDE -> leaves plan of every shape class of the stream, tuned before either arm runs (the
+    # plain arm's row LDE has no tuned choices); outside every timed region
+    t0 = time.perf_counter()
+    tuned = sum(zk.autotune(lg, r, b) > 0 for lg, b, _ in jobs)
+    t_tune = time.perf_counter() - t0
 
-    def plain_job(j):
-        lg, b, _ = jobs[j]
-        zk.fill_field(dev_in[: b << lg], seeds[j])
-        return plain.run(dev_in.data_ptr(), lg, r, b, ch)
+    def service_pass():
+        """Every job through the drop-in path, back to back in arrival order: per-job service times (input
+        generation included, as in a served job) and caps."""
+        dev_in = torch.empty(mx_in, dtype=torch.uint64, device="cuda")
+        # the LDE matrix of a job up to 60 GB; larger ones stream (leaves up to 80.5 GB beside it)
+        plain = DropIn(torch, zk.capi.LIB, zk.capi.check, mx_in, mx, mx_n, (60 << 30) // 8)
 
-    plain_job(0)
-    torch.cuda.synchronize()
-    service, caps_plain = [], []
-    with ClockSampler(torch.cuda.current_device()) as clk_plain:
-        for j in range(n_jobs):
-            t0 = time.perf_counter()
-            caps_plain.append(plain_job(j))
-            service.append(time.perf_counter() - t0)
-    cap_jobs_per_s = n_jobs / sum(service)
-    rng = np.random.default_rng(0x5EED0055)
-    arrivals = {f: np.cumsum(rng.exponential(1.0 / (f * cap_jobs_per_s), n_jobs)) for f in args.served_rates}
-    res = {"workload": f"served: first {n_jobs} jobs of the seeded 10,000-job stream (lg_n 12..22, polys 8..300, "
-                       "rate 3, cap_height 4, poseidon); inputs fill_field(job seed) generated on the device at "
-                       "each job's start (both arms)",
-           "jobs": n_jobs, "elems": elems, "plain_capacity_jobs_per_s": cap_jobs_per_s,
-           "plain_capacity_elems_per_s": elems / sum(service), "plain_streamed_jobs": plain.streamed,
-           "plain_service_s": {"p50": _pct(service, 50), "p99": _pct(service, 99), "max": max(service)},
-           "plain_service_clocks": clk_plain.summary(),
-           "slots": args.streams, "budget_gb": args.budget_gb, "rates": {}}
+        def plain_job(j):
+            lg, b, _ = jobs[j]
+            zk.fill_field(dev_in[: b << lg], seeds[j])
+            return plain.run(dev_in.data_ptr(), lg, r, b, ch)
 
-    replay = {}
-    if args.served_replay:
-        for f in args.served_rates:
-            lat = []
-            t0 = time.perf_counter()
-            for j, a in enumerate(arrivals[f]):
-                now = time.perf_counter() - t0
-                if now < a:
-                    time.sleep(a - now)
-                plain_job(j)
-                lat.append(time.perf_counter() - t0 - a)
-            replay[f] = (lat, time.perf_counter() - t0 - arrivals[f][0])
-    del plain, dev_in
-    torch.cuda.synchronize()
-    torch.cuda.empty_cache()
+        plain_job(0)
+        torch.cuda.synchronize()
+        service, caps = [], []
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            for j in range(n_jobs):
+                t0 = time.perf_counter()
+                caps.append(plain_job(j))
+                service.append(time.perf_counter() - t0)
+        return service, caps, clk.summary(), plain.streamed, plain_job, (plain, dev_in)
+
+    def served_run(arr):
+        with zk.Server(hbm_budget_bytes=args.budget_gb << 30, slots=args.streams) as srv:
+            lat_s, caps_s, errs, tick = {}, {}, [], {}
+
+            def client():  # completions in order; each tree released at once
+                try:
+                    while len(lat_s) < n_jobs:
+                        t = srv.wait_any(timeout_ms=1000)
+                        if t is not None:
+                            cap, lat = srv.wait(t)
+                            lat_s[t], caps_s[t] = lat, cap
+                            srv.release(t)
+                except Exception as e:  # noqa: BLE001 - reported by the main thread
+                    errs.append(e)
+
+            th = threading.Thread(target=client)
+            with ClockSampler(torch.cuda.current_device()) as clk:
+                th.start()
+                t0 = time.perf_counter()
+                for j, a in enumerate(arr):
+                    now = time.perf_counter() - t0
+                    if now < a:
+                        time.sleep(a - now)
+                    lg, b, _ = jobs[j]
+                    tick[j] = srv.submit_seeded(seeds[j], lg, b, r, ch)
+                th.join()
+            if errs:
+                raise errs[0]
+            span = time.perf_counter() - t0 - arr[0]
+            st = srv.stats()
+        lats = [lat_s[tick[j]] for j in range(n_jobs)]
+        caps = [caps_s[tick[j]] for j in range(n_jobs)]
+        return {"p50_s": _pct(lats, 50), "p99_s": _pct(lats, 99), "elems_per_s": elems / span,
+                "started_ahead": st["ahead"], "max_queue": st["max_queue"],
+                "hbm_peak_gb": st["hbm_peak"] / 2**30, "clocks": clk.summary()}, caps
+
+    arrivals, res, caps_ref = None, None, None
+    runs = {f: {"plain": [], "served": []} for f in args.served_rates}
     all_caps_ok = True
+    for rep in range(args.served_repeats):
+        service, caps_plain, clk_plain, streamed, plain_job, bufs = service_pass()
+        if arrivals is None:  # one arrival schedule for every repeat, from the first capacity measurement
+            cap_jobs_per_s = n_jobs / sum(service)
+            rng = np.random.default_rng(0x5EED0055)
+            arrivals = {f: np.cumsum(rng.exponential(1.0 / (f * cap_jobs_per_s), n_jobs))
+                        for f in args.served_rates}
+            caps_ref = caps_plain
+            res = {"workload": f"served: first {n_jobs} jobs of the seeded 10,000-job stream (lg_n 12..22, polys "
+                               "8..300, rate 3, cap_height 4, poseidon); inputs fill_field(job seed) generated on "
+                               "the device at each job's start (both arms)",
+                   "jobs": n_jobs, "elems": elems, "plain_capacity_jobs_per_s": cap_jobs_per_s,
+                   "plain_capacity_elems_per_s": elems / sum(service), "plain_streamed_jobs": streamed,
+                   "plain_service_s": {"p50": _pct(service, 50), "p99": _pct(service, 99), "max": max(service)},
+                   "plain_service_clocks": clk_plain,
+                   "slots": args.streams, "budget_gb": args.budget_gb, "autotuned_shape_classes": tuned,
+                   "autotune_s": t_tune, "repeats": args.served_repeats, "rates": {}}
+        all_caps_ok &= all(np.array_equal(x.reshape(-1), y.reshape(-1)) for x, y in zip(caps_plain, caps_ref))
+        for f in args.served_rates:
+            if args.served_replay:  # the FIFO queue in real time
+                lat = []
+                t0 = time.perf_counter()
+                for j, a in enumerate(arrivals[f]):
+                    now = time.perf_counter() - t0
+                    if now < a:
+                        time.sleep(a - now)
+                    plain_job(j)
+                    lat.append(time.perf_counter() - t0 - a)
+                lat_p, span_p = lat, time.perf_counter() - t0 - arrivals[f][0]
+            else:
+                lat_p, span_p = fifo_latencies(arrivals[f], service)
+            runs[f]["plain"].append({"p50_s": _pct(lat_p, 50), "p99_s": _pct(lat_p, 99), "elems_per_s": elems / span_p})
+        del bufs, plain_job
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        for f in args.served_rates:
+            one, caps_s = served_run(arrivals[f])
+            all_caps_ok &= all(np.array_equal(x.reshape(-1), y.reshape(-1)) for x, y in zip(caps_s, caps_ref))
+            runs[f]["served"].append(one)
+            print(json.dumps({"repeat": rep, "rate": f, "plain": runs[f]["plain"][-1], "served": one}),
+                  file=sys.stderr, flush=True)
+    med = lambda xs, k: float(np.median([x[k] for x in xs]))  # noqa: E731
     for f in args.served_rates:
-        lat_p, span_p = replay[f] if f in replay else fifo_latencies(arrivals[f], service)
-        runs = []
-        for rep in range(args.served_repeats):
-            with zk.Server(hbm_budget_bytes=args.budget_gb << 30, slots=args.streams) as srv:
-                lat_s, caps_s, errs = {}, {}, []
-                tick = {}
-
-                def client():  # completions in order; each tree released at once
-                    try:
-                        while len(lat_s) < n_jobs:
-                            t = srv.wait_any(timeout_ms=1000)
-                            if t is not None:
-                                cap, lat = srv.wait(t)
-                                lat_s[t], caps_s[t] = lat, cap
-                                srv.release(t)
-                    except Exception as e:  # noqa: BLE001 - reported by the main thread
-                        errs.append(e)
-
-                th = threading.Thread(target=client)
-                with ClockSampler(torch.cuda.current_device()) as clk:
-                    th.start()
-                    t0 = time.perf_counter()
-                    for j, a in enumerate(arrivals[f]):
-                        now = time.perf_counter() - t0
-                        if now < a:
-                            time.sleep(a - now)
-                        lg, b, _ = jobs[j]
-                        tick[j] = srv.submit_seeded(seeds[j], lg, b, r, ch)
-                    th.join()
-                if errs:
-                    raise errs[0]
-                span = time.perf_counter() - t0 - arrivals[f][0]
-                st = srv.stats()
-            ok = all(np.array_equal(caps_s[tick[j]].reshape(-1), caps_plain[j].reshape(-1)) for j in range(n_jobs))
-            all_caps_ok &= ok
-            lats = [lat_s[tick[j]] for j in range(n_jobs)]
-            runs.append({"p50_s": _pct(lats, 50), "p99_s": _pct(lats, 99), "elems_per_s": elems / span,
-                         "started_ahead": st["ahead"], "max_queue": st["max_queue"],
-                         "hbm_peak_gb": st["hbm_peak"] / 2**30, "clocks": clk.summary()})
-        med = lambda k: float(np.median([x[k] for x in runs]))  # noqa: E731
+        P, S = runs[f]["plain"], runs[f]["served"]
         entry = {
-            "arrival_jobs_per_s": f * cap_jobs_per_s,
-            "plain": {"p50_s": _pct(lat_p, 50), "p99_s": _pct(lat_p, 99), "elems_per_s": elems / span_p,
-                      "how": "real-time replay" if f in replay else "FIFO over measured service times"},
-            "served": {"p50_s": med("p50_s"), "p99_s": med("p99_s"), "elems_per_s": med("elems_per_s"),
-                       "started_ahead": int(med("started_ahead")), "max_queue": int(med("max_queue")),
-                       "hbm_peak_gb": med("hbm_peak_gb"), "clocks": runs[len(runs) // 2]["clocks"]},
+            "arrival_jobs_per_s": f * res["plain_capacity_jobs_per_s"],
+            "plain": {"p50_s": med(P, "p50_s"), "p99_s": med(P, "p99_s"), "elems_per_s": med(P, "elems_per_s"),
+                      "how": "real-time replay of the FIFO queue" if args.served_replay
+                      else "FIFO queue over the measured per-job service times"},
+            "served": {"p50_s": med(S, "p50_s"), "p99_s": med(S, "p99_s"), "elems_per_s": med(S, "elems_per_s"),
+                       "started_ahead": int(med(S, "started_ahead")), "max_queue": int(med(S, "max_queue")),
+                       "hbm_peak_gb": med(S, "hbm_peak_gb"), "clocks": S[len(S) // 2]["clocks"]},
         }
-        if len(runs) > 1:
-            entry["served"]["runs"] = runs
         entry["served_over_plain"] = {"p50": entry["plain"]["p50_s"] / entry["served"]["p50_s"],
                                       "p99": entry["plain"]["p99_s"] / entry["served"]["p99_s"],
                                       "elems_per_s": entry["served"]["elems_per_s"] / entry["plain"]["elems_per_s"]}
+        if len(S) > 1:  # run-to-run spread, both arms
+            entry["runs"] = {"plain": [{k: x[k] for k in ("p50_s", "p99_s", "elems_per_s")} for x in P],
+                             "served": [{k: x[k] for k in ("p50_s", "p99_s", "elems_per_s")} for x in S]}
         res["rates"][str(f)] = entry
-        print(json.dumps({"rate": f, **entry}), file=sys.stderr, flush=True)
     res["check"] = {"served_caps_equal_plain": bool(all_caps_ok)}
     if baseline_legs:
         small = sorted(range(n_jobs), key=lambda j: jobs[j][1] << jobs[j][0])[: args.oracle_sample]
         want = _oracle_caps([(seeds[j], jobs[j][0], jobs[j][1], r) for j in small])
-        res["check"]["sample_caps_equal_oracle"] = all(np.array_equal(caps_plain[j].reshape(-1), w.reshape(-1))
+        res["check"]["sample_caps_equal_oracle"] = all(np.array_equal(caps_ref[j].reshape(-1), w.reshape(-1))
                                                        for j, w in zip(small, want))
     return res
 

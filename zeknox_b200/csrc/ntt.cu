@@ -755,7 +755,8 @@ int ntt_autotune_leaves(uint32_t lg_n, uint32_t rate_bits, uint64_t batches, cud
     DeviceCtx &ctx = device_ctx(current_device());
     const uint64_t N = 1ull << lg, n = 1ull << lg_n;
     // a representative batch: the class's own size, capped at ~1 GiB of leaves
-    const uint64_t bt = std::max<uint64_t>(1, std::min<uint64_t>(batches, (1ull << 27) / N));
+    // but never below the 8 polynomials a chunk of the leaves stage holds
+    const uint64_t bt = std::max<uint64_t>(1, std::min<uint64_t>(batches, std::max<uint64_t>(8, (1ull << 27) / N)));
     Scratch in(bt * n * sizeof(uint64_t), s), out(bt * N * sizeof(uint64_t), s);
     const uint64_t scr_elems = ntt_leaves_scratch_elems(lg, bt);
     Scratch scr(scr_elems * sizeof(uint64_t), s);
