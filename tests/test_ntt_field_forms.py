@@ -1,10 +1,11 @@
-"""The NTT's field operations (zeknox_b200/csrc/ntt.cu: nt_sub, nt_add,
-nt_canon, nt_reduce128 and the x 2^24 fold of gl_mul2_24) are PTX carry-flag
-sequences.  Each is replayed here instruction by instruction with PTX's CC.CF
-semantics (add.cc / addc carry, sub.cc / subc borrow, mad.lo.cc /
-madc.hi.cc) and checked exactly against the field on random and edge-case
-operands.  The GPU parity tests pin the compiled kernels' outputs; this pins
-the algebra of each sequence."""
+"""Field operations written as PTX carry sequences: the NTT's nt_sub, nt_add,
+nt_canon, nt_reduce128 and the x 2^24 fold of gl_mul2_24 (ntt_field.cuh), and
+the hash S-box's sqr_wide (gl64.cuh).  Each is replayed here instruction by
+instruction with PTX's CC.CF semantics (add.cc / addc carry, sub.cc / subc
+borrow, mad.lo.cc / madc.hi.cc, shf.l.wrap) and checked exactly against the
+field (or the integer square) on random and edge-case operands.  The GPU
+parity tests pin the compiled kernels' outputs; this pins the algebra of each
+sequence."""
 
 import random
 
@@ -160,3 +161,27 @@ def test_extreme_128_bit_inputs():
     for v in [(2**64 - 1) ** 2, 2**128 - 1, 0, 2**96, 2**96 - 1, P * (2**64 - 1)]:
         r = nt_reduce128(v & M32, (v >> 32) & M32, (v >> 64) & M32, v >> 96)
         assert r % P == v % P and nt_canon(r) == v % P
+
+
+def sqr_wide(a):
+    """gl64.cuh sqr_wide: a^2 from a0^2, a1^2 and the cross term a0 a1, doubled
+    by a funnel shift (shf.l.wrap) and added once."""
+    f = Flags()
+    a0, a1 = halves(a)
+    r0, r1 = (a0 * a0) & M32, (a0 * a0) >> 32
+    r2, r3 = (a1 * a1) & M32, (a1 * a1) >> 32
+    c0, c1 = (a0 * a1) & M32, (a0 * a1) >> 32
+    c2 = c1 >> 31
+    c1 = ((c1 << 1) | (c0 >> 31)) & M32  # shf.l.wrap.b32 c1, c0, c1, 1
+    c0 = (c0 << 1) & M32
+    r1 = f.add_cc(r1, c0)
+    r2 = f.addc_cc(r2, c1)
+    r3 = f.addc(r3, c2)
+    return r0 | (r1 << 32) | (r2 << 64) | (r3 << 96)
+
+
+def test_sqr_wide_is_the_exact_square():
+    rnd = random.Random(11)
+    edge = [0, 1, M32, M32 + 1, 2**63, 2**64 - 1, P - 1, P, 0x80000000, 0xFFFFFFFF80000000]
+    for a in edge + [rnd.getrandbits(64) for _ in range(20000)]:
+        assert sqr_wide(a) == a * a, hex(a)

@@ -158,6 +158,7 @@ __device__ __forceinline__ void smem_dif(uint64_t *sm, const uint64_t *tw, uint3
     }
 }
 
+template <bool INV>
 __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
     extern __shared__ uint64_t smem[];
     const uint32_t l = a.l, L = 1u << l;
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
             for (uint32_t b = 1; b < (1u << rr); b++)
                 sm[((b << lv) + e) * tp + t] = nt_mul(v, tw[(e * brev_bits(b, rr)) & (L - 1)]);
         }
-        smem_dif(sm, tw, l, (int)lv - 1, a.lg_t, tp, a.inverse != 0);
+        smem_dif(sm, tw, l, (int)lv - 1, a.lg_t, tp, INV);
         // store with the inter-pass twiddle w_N^((r0 + t) k Q): one table load
         // each, or (no one-load table) stepped by k with a second product
         const uint32_t t = threadIdx.x & (T - 1);
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
         sm[e * tp + t] = v;
     }
     cp_async_wait_all();
-    smem_dif(sm, tw, l, (int)l - 1, a.lg_t, tp, a.inverse != 0);
+    smem_dif(sm, tw, l, (int)l - 1, a.lg_t, tp, INV);
     if (a.kind == 1) {
         // natural index of line t's element k: krev + Q * k
         uint64_t *dst = a.dst + poly0 * a.dst_poly_stride;
@@ -322,6 +323,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_pass_kernel(PassArgs a) {
 // the same prefix (line krev) of 2^lg_t consecutive polynomials, so that every
 // leaf row receives 2^lg_t contiguous elements.  Element k of line krev has
 // natural index o = krev + Q k and goes to dst[rev_lg(o) * leaf_stride + b].
+template <bool INV>
 __global__ void __launch_bounds__(kNttThreads) ntt_last_pass_leaves(PassArgs a) {
     extern __shared__ uint64_t smem[];
     const uint32_t l = a.l, L = 1u << l;
@@ -343,7 +345,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_last_pass_leaves(PassArgs a) 
         else sm[e * tp + p] = 0ull;
     }
     cp_async_wait_all();
-    smem_dif(sm, tw, l, (int)l - 1, a.lg_t, tp, a.inverse != 0);
+    smem_dif(sm, tw, l, (int)l - 1, a.lg_t, tp, INV);
     const uint32_t lg = a.lg_n;
     for (uint32_t idx = threadIdx.x; idx < P * L; idx += blockDim.x) {
         const uint32_t p = idx & (P - 1), k = idx >> a.lg_t;
@@ -458,20 +460,24 @@ size_t pass_smem(uint32_t l, uint32_t lg_t) {
 
 // after_pass: the previous launch on `s` is the pass before this one of the
 // same transform, so this pass may start while it drains (pdl.cuh).
+// The transform's direction is a template parameter of the pass kernels (the
+// 8-point DFT's root multiplies differ), so each compiled kernel holds one form.
 void launch_pass(const PassArgs &a, uint64_t groups, cudaStream_t s, bool after_pass) {
     const size_t smem = pass_smem(a.l, a.lg_t);
     static std::atomic<uint64_t> attr_set{0};  // one bit per device
     const int dev = current_device();
     if (dev < 64 && !(attr_set.load() & (1ull << dev))) {
-        ZK_CUDA(cudaFuncSetAttribute(ntt_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        ZK_CUDA(cudaFuncSetAttribute(ntt_pass_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        ZK_CUDA(cudaFuncSetAttribute(ntt_pass_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
         attr_set.fetch_or(1ull << dev);
     }
     require(groups < (1ull << 31), "transform too large for one launch");
+    auto kern = a.inverse ? ntt_pass_kernel<true> : ntt_pass_kernel<false>;
     if (after_pass) {
-        launch_after(ntt_pass_kernel, (unsigned)groups, kNttThreads, smem, s, a);
+        launch_after(kern, (unsigned)groups, kNttThreads, smem, s, a);
         return;
     }
-    ntt_pass_kernel<<<(unsigned)groups, kNttThreads, smem, s>>>(a);
+    kern<<<(unsigned)groups, kNttThreads, smem, s>>>(a);
     ZK_CHECK_LAUNCH();
 }
 
@@ -480,11 +486,13 @@ void launch_leaves_pass(const PassArgs &a, uint64_t groups, cudaStream_t s) {
     static std::atomic<uint64_t> attr_set{0};
     const int dev = current_device();
     if (dev < 64 && !(attr_set.load() & (1ull << dev))) {
-        ZK_CUDA(cudaFuncSetAttribute(ntt_last_pass_leaves, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        ZK_CUDA(cudaFuncSetAttribute(ntt_last_pass_leaves<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     160 * 1024));
         attr_set.fetch_or(1ull << dev);
     }
     require(groups < (1ull << 31), "transform too large for one launch");
-    launch_after(ntt_last_pass_leaves, (unsigned)groups, kNttThreads, smem, s, a);  // always after a pass
+    require(!a.inverse, "the leaf layout is written by forward transforms only");
+    launch_after(ntt_last_pass_leaves<false>, (unsigned)groups, kNttThreads, smem, s, a);  // always after a pass
 }
 
 }  // namespace
