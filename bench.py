@@ -286,7 +286,8 @@ def main() -> None:
     ap.add_argument("--rate-bits", type=int, default=3)
     ap.add_argument("--cap-height", type=int, default=4)
     ap.add_argument("--hash", default="poseidon", choices=sorted(HASH_NAMES))
-    ap.add_argument("--workload", default="commit", choices=["commit", "merkle", "sweep", "batched", "served", "fri"],
+    ap.add_argument("--workload", default="commit",
+                    choices=["commit", "merkle", "sweep", "batched", "served", "fri", "field-ops", "tensor-bound"],
                     help="commit (default, the bench line); the others print their own JSON summary")
     ap.add_argument("--leaves", type=int, default=8192, help="leaf count of the merkle workload (a power of two)")
     ap.add_argument("--streams", type=int, default=4, help="internal streams of a batch / slots of the server")
@@ -304,7 +305,7 @@ def main() -> None:
     args = ap.parse_args()
     if args.workload != "commit" and args.impl == "ours":
         {"merkle": run_merkle_only, "sweep": run_sweep, "batched": run_batched, "served": run_served,
-         "fri": run_fri}[args.workload](args)
+         "fri": run_fri, "field-ops": run_field_ops, "tensor-bound": run_tensor_bound}[args.workload](args)
         return
     set_workload(args.polys, args.lg_n, args.rate_bits, args.cap_height, args.hash)
     if args.impl == "reference":
@@ -1126,6 +1127,70 @@ def served_section(args, zk, torch, baseline_legs: bool) -> dict:
         res["check"]["sample_caps_equal_oracle"] = all(np.array_equal(caps_ref[j].reshape(-1), w.reshape(-1))
                                                        for j, w in zip(small, want))
     return res
+
+
+def run_field_ops(args):
+    """One launch per field operation (libzkprobe.so), for counting instructions per operation under ncu:
+    the kernel's count minus probe_base's (probe_dft8: minus probe_dft8_base's), divided by the iterations."""
+    import ctypes
+
+    lib = ctypes.CDLL(str(ROOT / "zeknox_b200" / "libzkprobe.so"))
+    iters = 4096
+    r = lib.zk_probe_field_ops(iters)
+    assert r == 0, r
+    print(json.dumps({"workload": "field-ops", "iterations": iters}), flush=True)
+
+
+def run_tensor_bound(args):
+    """What an int8 tensor-core formulation would cost in its GEMM alone, measured with the library int8
+    GEMM (cuBLASLt through torch._int_mm: int8 x int8 -> int32), at the shapes the default commit needs:
+
+    * LDE: a 64-point DFT over byte limbs.  A line of 64 elements is 64 x 8 bytes (K = 512); the DFT matrix's
+      entries are powers of two, so each output element needs 12 partial sums (one per byte position of a
+      96-bit result, 2^96 = -1 folding the rest): N = 64 x 12 = 768.  The 135 x 2^18 output is 552,960 lines
+      per 64-point level, and the transform has three such levels.
+    * Poseidon: the MDS layer of one round over byte limbs of the 12 lanes (K = 96, N = 96) for the
+      4,456,448 leaf permutations; a permutation has 30 rounds.
+
+    Both GEMMs write their int32 partial sums to HBM here; a fused kernel would keep them in TMEM, so the
+    GEMM time is the compute floor of each formulation, before its recombination arithmetic.  Beside each:
+    the SIMT kernel's measured time for the same work in the default commit."""
+    import torch
+
+    import zeknox_b200 as zk
+
+    def ev(fn, reps=10):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    out = {"workload": "tensor-core bound: int8 GEMMs of the byte-limb formulations (cuBLASLt via torch._int_mm)"}
+    g = torch.Generator(device="cuda").manual_seed(1)
+    for name, (m, k, n, reps_per_commit) in {"lde_dft64_level": (552960, 512, 768, 3),
+                                             "poseidon_mds_round": (4456448, 96, 96, 30)}.items():
+        a = torch.randint(-128, 127, (m, k), generator=g, device="cuda", dtype=torch.int8)
+        b = torch.randint(-128, 127, (k, n), generator=g, device="cuda", dtype=torch.int8)
+        try:
+            torch._int_mm(a, b)
+        except RuntimeError:  # some builds want the second operand column-major
+            b = b.t().contiguous().t()
+        ms = ev(lambda: torch._int_mm(a, b))
+        out[name] = {"m": m, "k": k, "n": n, "gemm_ms": ms, "tops": 2 * m * k * n / (ms * 1e-3) / 1e12,
+                     "per_commit": reps_per_commit, "gemm_ms_per_commit": ms * reps_per_commit}
+        del a, b
+        torch.cuda.empty_cache()
+    x = zk.fill_field(torch.empty(135 << 15, dtype=torch.uint64, device="cuda"), 7).view(135, 1 << 15)
+    lv = torch.empty((1 << 18, 135), dtype=torch.uint64, device="cuda")
+    out["simt_lde_to_leaves_ms"] = ev(lambda: zk.lde_leaves(x, 3, out=lv))
+    d, c = zk.merkle_tree(lv, 4, 0)
+    out["simt_merkle_ms"] = ev(lambda: zk.merkle_tree(lv, 4, 0, d, c))
+    print(json.dumps(out), flush=True)
 
 
 def run_batched(args):

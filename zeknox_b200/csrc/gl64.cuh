@@ -202,22 +202,23 @@ __device__ __forceinline__ uint64_t pr_add_c(uint64_t a, uint64_t c) {
 // (Poseidon 2^18 x 135 tree 4.342 -> 4.308 ms, Poseidon2 4.398 -> 4.309 ms).
 __device__ __forceinline__ void sqr_wide(uint64_t a, uint64_t &lo, uint64_t &hi) {
     const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
-    uint32_t r0, r1, r2, r3, c0, c1, c2;
+    uint32_t r0, r1, r2, r3;
     asm("{\n\t"
-        "mul.lo.u32 %0, %7, %7;\n\t"
-        "mul.hi.u32 %1, %7, %7;\n\t"
-        "mul.lo.u32 %2, %8, %8;\n\t"
-        "mul.hi.u32 %3, %8, %8;\n\t"
-        "mul.lo.u32 %4, %7, %8;\n\t"
-        "mul.hi.u32 %5, %7, %8;\n\t"
-        "shr.u32 %6, %5, 31;\n\t"              // bit 64 of 2 a0 a1
-        "shf.l.wrap.b32 %5, %4, %5, 1;\n\t"
-        "shl.b32 %4, %4, 1;\n\t"
-        "add.cc.u32 %1, %1, %4;\n\t"
-        "addc.cc.u32 %2, %2, %5;\n\t"
-        "addc.u32 %3, %3, %6;\n\t"
+        ".reg .u32 c0, c1, c2;\n\t"
+        "mul.lo.u32 %0, %4, %4;\n\t"
+        "mul.hi.u32 %1, %4, %4;\n\t"
+        "mul.lo.u32 %2, %5, %5;\n\t"
+        "mul.hi.u32 %3, %5, %5;\n\t"
+        "mul.lo.u32 c0, %4, %5;\n\t"
+        "mul.hi.u32 c1, %4, %5;\n\t"
+        "shr.u32 c2, c1, 31;\n\t"              // bit 64 of 2 a0 a1
+        "shf.l.wrap.b32 c1, c0, c1, 1;\n\t"
+        "shl.b32 c0, c0, 1;\n\t"
+        "add.cc.u32 %1, %1, c0;\n\t"
+        "addc.cc.u32 %2, %2, c1;\n\t"
+        "addc.u32 %3, %3, c2;\n\t"
         "}"
-        : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3), "=r"(c0), "=r"(c1), "=r"(c2)
+        : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
         : "r"(a0), "r"(a1));
     lo = ((uint64_t)r1 << 32) | r0;
     hi = ((uint64_t)r3 << 32) | r2;

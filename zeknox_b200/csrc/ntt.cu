@@ -17,6 +17,7 @@
 // remaining passes transform each contiguous block of S_1 elements the same
 // way, and the last pass stores X at its natural index.
 #include <stdint.h>
+#include <stdlib.h>
 
 #include <algorithm>
 #include <atomic>
@@ -156,6 +157,83 @@ __device__ __forceinline__ void smem_dif(uint64_t *sm, const uint64_t *tw, uint3
         }
         __syncthreads();
     }
+}
+
+// smem_dif with the line length (2^LG_L), the lines per block (2^LG_T), the
+// first half-span (S) and the direction fixed at compile time: the unit loops
+// unroll and every index but the thread's own folds to a constant.  Same
+// steps and synchronisation as smem_dif.
+template <int LG_L, int LG_T, int S, bool INV>
+__device__ __forceinline__ void smem_dif_fixed(uint64_t *sm, const uint64_t *tw) {
+    constexpr uint32_t T = 1u << LG_T, TP = T > 1 ? T + 1 : 1;
+    if constexpr (S >= 2) {
+        constexpr uint32_t LQ = S - 2, Q = 1u << LQ, SH8 = LG_L - 1 - S;
+        constexpr uint32_t UNITS = T << (LG_L - 3);
+        __syncthreads();
+#pragma unroll
+        for (uint32_t it = 0; it < (UNITS + kNttThreads - 1) / kNttThreads; it++) {
+            const uint32_t u = threadIdx.x + it * kNttThreads;
+            if (UNITS % kNttThreads == 0 || u < UNITS) {
+                const uint32_t t = u & (T - 1), w = u >> LG_T;
+                const uint32_t o = w & (Q - 1), e0 = ((w >> LQ) << (LQ + 3)) + o;
+                uint64_t *b = sm + e0 * TP + t;
+                uint64_t x[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++) x[k] = b[k * Q * TP];
+                dft8(x, INV);
+                if constexpr (LQ > 0) {
+                    if (o != 0) {
+                        constexpr uint32_t rev3[8] = {0, 4, 2, 6, 1, 5, 3, 7};
+#pragma unroll
+                        for (int j = 1; j < 8; j++) x[j] = nt_mul(x[j], tw[(o * rev3[j]) << SH8]);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 8; k++) b[k * Q * TP] = x[k];
+            }
+        }
+        smem_dif_fixed<LG_L, LG_T, S - 3, INV>(sm, tw);
+    } else {
+        __syncthreads();
+        if constexpr (S == 1) {  // spans 2 and 1: radix-4 units
+            constexpr uint32_t UNITS = T << (LG_L - 2);
+#pragma unroll
+            for (uint32_t it = 0; it < (UNITS + kNttThreads - 1) / kNttThreads; it++) {
+                const uint32_t u = threadIdx.x + it * kNttThreads;
+                if (UNITS % kNttThreads == 0 || u < UNITS) {
+                    uint64_t *b = sm + ((u >> LG_T) << 2) * TP + (u & (T - 1));
+                    const uint64_t x0 = b[0], x1 = b[TP], x2 = b[2 * TP], x3 = b[3 * TP];
+                    const uint64_t a0 = nt_add(x0, x2), a2 = nt_sub(x0, x2), a1 = nt_add(x1, x3);
+                    const uint64_t a3 = INV ? gl_mul2_48(nt_sub(x3, x1)) : gl_mul2_48(nt_sub(x1, x3));
+                    b[0] = nt_add(a0, a1);
+                    b[TP] = nt_sub(a0, a1);
+                    b[2 * TP] = nt_add(a2, a3);
+                    b[3 * TP] = nt_sub(a2, a3);
+                }
+            }
+            __syncthreads();
+        } else if constexpr (S == 0) {  // span 1
+            constexpr uint32_t UNITS = T << (LG_L - 1);
+#pragma unroll
+            for (uint32_t it = 0; it < (UNITS + kNttThreads - 1) / kNttThreads; it++) {
+                const uint32_t u = threadIdx.x + it * kNttThreads;
+                if (UNITS % kNttThreads == 0 || u < UNITS) {
+                    uint64_t *b = sm + ((u >> LG_T) << 1) * TP + (u & (T - 1));
+                    uint64_t x0 = b[0], x1 = b[TP];
+                    bfly1(x0, x1);
+                    b[0] = x0;
+                    b[TP] = x1;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__host__ __device__ constexpr uint32_t brev_const(uint32_t x, int bits) {
+    uint32_t r = 0;
+    for (int i = 0; i < bits; i++) r |= ((x >> i) & 1u) << (bits - 1 - i);
+    return r;
 }
 
 template <bool INV>
@@ -357,6 +435,190 @@ __global__ void __launch_bounds__(kNttThreads) ntt_last_pass_leaves(PassArgs a) 
 }
 
 
+using PassKernel = void (*)(PassArgs);
+
+// The column pass (kind 0) of ntt_pass_kernel with the line length (2^LG_L),
+// lines per block (2^LG_T) and non-zero prefix of every line (2^LV, LV ==
+// LG_L: no zero extension) fixed at compile time, for launches with the
+// one-load twiddle table and, when there is a coset, the one-load coset table
+// (transforms of up to 2^20 points).  Thread t's elements are t + 256 j: its
+// line (t mod T) is fixed, and its element and output positions step by
+// constants.
+template <int LG_L, int LG_T, int LV, bool INV>
+__global__ void __launch_bounds__(kNttThreads) ntt_column_fixed(PassArgs a) {
+    constexpr uint32_t L = 1u << LG_L, T = 1u << LG_T, TP = T > 1 ? T + 1 : 1, RR = LG_L - LV;
+    static_assert(RR == 0 || RR >= 2, "a one-stage zero extension takes the generic pass");
+    static_assert(T <= kNttThreads && (T << LG_L) % kNttThreads == 0, "block elements: a multiple of the threads");
+    extern __shared__ uint64_t smem[];
+    uint64_t *tw = smem;  // omega_L^e, e < L
+    uint64_t *sm = smem + L;
+    for (uint32_t j = threadIdx.x; j < L; j += kNttThreads) tw[j] = __ldg(a.line_roots + (j << (kLineLgMax - LG_L)));
+    pdl_wait();
+    const uint32_t lg_s = a.lg_s, lg_gpp = lg_s - LG_T;  // groups per prefix: 2^lg_gpp
+    const uint64_t g = blockIdx.x;
+    const uint64_t poly = g >> (lg_gpp + a.lg_pre);
+    const uint64_t rem = g & ((1ull << (lg_gpp + a.lg_pre)) - 1);
+    const uint64_t base = (rem >> lg_gpp) << (LG_L + lg_s);  // prefix block start within the polynomial
+    const uint32_t t = threadIdx.x & (T - 1);
+    const uint64_t r = ((rem & ((1ull << lg_gpp) - 1)) << LG_T) + t;  // this thread's line
+    const uint64_t *src = a.src + poly * a.src_poly_stride + base + r;  // element e of the line: src[e << lg_s]
+    uint64_t *dst = a.dst + poly * a.dst_poly_stride + base + r;
+    const uint64_t i0 = base + r;  // index within the polynomial of the line's element 0
+    const uint32_t e0 = threadIdx.x >> LG_T;
+    constexpr uint32_t DE = kNttThreads >> LG_T;  // element step between j and j + 1
+    const uint64_t *pre = a.pre_full;
+    __syncthreads();  // the twiddle table, read by the replication below
+    if constexpr (RR >= 2) {
+        // inputs (line block 1) and coset powers (line block 2) staged with asynchronous copies;
+        // each thread reads back only the slots it staged, before its replication overwrites them
+        constexpr uint32_t NE = (T << LV) < kNttThreads ? 1 : (T << LV) / kNttThreads;
+        if ((T << LV) >= kNttThreads || threadIdx.x < (T << LV)) {
+#pragma unroll
+            for (uint32_t j = 0; j < NE; j++) {
+                const uint32_t e = e0 + j * DE;
+                const uint64_t i = i0 + ((uint64_t)e << lg_s);
+                if (i < a.n_valid) {
+                    cp_async8(&sm[((1u << LV) + e) * TP + t], src + ((uint64_t)e << lg_s));
+                    if (pre) cp_async8(&sm[((2u << LV) + e) * TP + t], pre + i);
+                }
+            }
+        }
+        cp_async_wait_all();
+        if ((T << LV) >= kNttThreads || threadIdx.x < (T << LV)) {
+#pragma unroll
+            for (uint32_t j = 0; j < NE; j++) {
+                const uint32_t e = e0 + j * DE;
+                const uint64_t i = i0 + ((uint64_t)e << lg_s);
+                uint64_t v = 0;
+                if (i < a.n_valid) {
+                    v = nt_canon(sm[((1u << LV) + e) * TP + t]);
+                    if (pre) v = nt_mul(v, sm[((2u << LV) + e) * TP + t]);
+                }
+                sm[e * TP + t] = v;
+#pragma unroll
+                for (uint32_t b = 1; b < (1u << RR); b++)
+                    sm[((b << LV) + e) * TP + t] = nt_mul(v, tw[(e * brev_const(b, RR)) & (L - 1)]);
+            }
+        }
+    } else {
+#pragma unroll
+        for (uint32_t j = 0; j < (T << LG_L) / kNttThreads; j++) {
+            const uint32_t e = e0 + j * DE;
+            const uint64_t i = i0 + ((uint64_t)e << lg_s);
+            uint64_t v = 0;
+            if (i < a.n_valid) {
+                v = nt_canon(src[(uint64_t)e << lg_s]);
+                if (pre) v = nt_mul(v, __ldg(pre + i));
+            }
+            sm[e * TP + t] = v;
+        }
+    }
+    smem_dif_fixed<LG_L, LG_T, (int)LV - 1, INV>(sm, tw);
+    // store with the inter-pass twiddle w_N^(r k Q), one table load each (the
+    // table has N <= 2^20 entries, so exponents wrap mod 2^32 harmlessly)
+    const uint32_t nmask = (uint32_t)((1ull << a.lg_n) - 1);
+    const uint32_t krt = __brev(e0) >> (32 - LG_L);  // rev(k) of the first k = e0
+    const uint32_t rk0 = (uint32_t)r * e0, rdk = (uint32_t)r * DE;
+    const uint32_t lg_pre = a.lg_pre;
+    const uint64_t *twf = a.tw_full;
+#pragma unroll
+    for (uint32_t m = 0; m < (T << LG_L) / kNttThreads; m++) {
+        const uint32_t k = e0 + m * DE;
+        const uint32_t kr = krt | brev_const(m * DE, LG_L);
+        const uint64_t tw_k = __ldg(twf + (((rk0 + m * rdk) << lg_pre) & nmask));
+        dst[(uint64_t)k << lg_s] = nt_mul(sm[kr * TP + t], tw_k);
+    }
+}
+
+// The compiled (line length, lines per block, non-zero prefix) triples of
+// ntt_column_fixed, per direction.
+template <bool INV>
+PassKernel column_fixed_kernel(uint32_t l, uint32_t lg_t, uint32_t lv) {
+#define ZK_COLUMN_CASES(LG_L, LG_T)                                                        \
+    case ((LG_L) << 8 | (LG_T) << 4 | 0): return ntt_column_fixed<LG_L, LG_T, LG_L, INV>;      \
+    case ((LG_L) << 8 | (LG_T) << 4 | 2): return ntt_column_fixed<LG_L, LG_T, LG_L - 2, INV>;  \
+    case ((LG_L) << 8 | (LG_T) << 4 | 3): return ntt_column_fixed<LG_L, LG_T, LG_L - 3, INV>;
+    if (lv > l) return nullptr;
+    switch (l << 8 | lg_t << 4 | (l - lv)) {
+        ZK_COLUMN_CASES(7, 5) ZK_COLUMN_CASES(8, 5) ZK_COLUMN_CASES(9, 4) ZK_COLUMN_CASES(10, 3)
+        ZK_COLUMN_CASES(11, 2) ZK_COLUMN_CASES(12, 1)
+        default: return nullptr;
+    }
+#undef ZK_COLUMN_CASES
+}
+
+// ntt_last_pass_leaves with the line length (2^LG_L) and polynomials per
+// block (2^LG_P) fixed at compile time, for blocks whose P * L elements are a
+// multiple of the thread count: thread t's elements are t + 256 i, so their
+// polynomial, line position and leaf row split into a part of t, computed
+// once, and a part of i, a constant.  A line element k goes to the leaf row
+// rev_lg(krev + Q k) = (rev_lg_pre(krev) << LG_L) | rev_LG_L(k).
+template <int LG_L, int LG_P>
+__global__ void __launch_bounds__(kNttThreads) ntt_leaves_fixed(PassArgs a) {
+    constexpr uint32_t L = 1u << LG_L, P = 1u << LG_P, TP = P > 1 ? P + 1 : 1;
+    constexpr uint32_t PER = P * L / kNttThreads;  // elements per thread
+    static_assert(P * L % kNttThreads == 0 && LG_P <= 8, "block elements: a multiple of the thread count");
+    extern __shared__ uint64_t smem[];
+    uint64_t *tw = smem;
+    uint64_t *sm = smem + L;
+    for (uint32_t j = threadIdx.x; j < L; j += kNttThreads) tw[j] = __ldg(a.line_roots + (j << (kLineLgMax - LG_L)));
+    pdl_wait();  // the previous pass's output is read only from here on
+    const uint32_t lg_pre = a.lg_pre;
+    const uint64_t krev = blockIdx.x & ((1ull << lg_pre) - 1), p0 = (uint64_t)(blockIdx.x >> lg_pre) << LG_P;
+    const uint32_t np = (uint32_t)min((uint64_t)P, a.batches - p0);
+    const uint64_t mask1 = (1ull << a.l_first) - 1;
+    const uint64_t kpos = ((krev & mask1) << (lg_pre - a.l_first)) | (krev >> a.l_first);
+    const uint64_t stride = a.src_poly_stride;
+    const uint64_t *src = a.src + p0 * stride + (kpos << LG_L);
+#pragma unroll
+    for (uint32_t i = 0; i < PER; i++) {
+        uint32_t e, p;  // element t + 256 i: line position e of polynomial p
+        if constexpr (LG_L >= 8) {
+            e = threadIdx.x + kNttThreads * (i & (L / kNttThreads - 1));
+            p = i / (L / kNttThreads);
+        } else {
+            e = threadIdx.x & (L - 1);
+            p = (threadIdx.x >> LG_L) + i * (kNttThreads >> LG_L);
+        }
+        if (p < np) cp_async8(&sm[e * TP + p], src + p * stride + e);
+        else sm[e * TP + p] = 0ull;
+    }
+    cp_async_wait_all();
+    smem_dif_fixed<LG_L, LG_P, LG_L - 1, false>(sm, tw);
+    // stores: element t + 256 i is polynomial p = t mod P at line position
+    // k = t / P + i * (256 / P), whose bit-reversal is rev(t / P) | rev(i * 256 / P)
+    const uint32_t p = threadIdx.x & (P - 1);
+    if (p >= np) return;
+    const uint32_t kt = threadIdx.x >> LG_P;
+    const uint32_t krt = __brev(kt) >> (32 - LG_L);
+    const uint64_t ls = a.leaf_stride;
+    uint64_t *dst = a.dst + p0 + p + (((uint64_t)brev_bits((uint32_t)krev, lg_pre) << LG_L) | krt) * ls;
+    const uint64_t *col = sm + p;
+#pragma unroll
+    for (uint32_t i = 0; i < PER; i++) {
+        constexpr uint32_t KS = 8 - LG_P;  // log2 of the step of k between i and i + 1
+        const uint32_t kri = brev_const(i << KS, LG_L);  // a constant for each i
+        dst[(uint64_t)kri * ls] = col[(krt | kri) * TP];
+    }
+}
+
+// The compiled (line length, polynomials per block) pairs of ntt_leaves_fixed.
+#define ZK_LEAVES_CASE(LG_L, LG_P) \
+    case ((LG_L) << 4 | (LG_P)): return ntt_leaves_fixed<LG_L, LG_P>;
+PassKernel leaves_fixed_kernel(uint32_t l, uint32_t lg_t) {
+    switch (l << 4 | lg_t) {
+        ZK_LEAVES_CASE(6, 2) ZK_LEAVES_CASE(6, 3) ZK_LEAVES_CASE(6, 4)
+        ZK_LEAVES_CASE(7, 1) ZK_LEAVES_CASE(7, 2) ZK_LEAVES_CASE(7, 3) ZK_LEAVES_CASE(7, 4)
+        ZK_LEAVES_CASE(8, 0) ZK_LEAVES_CASE(8, 1) ZK_LEAVES_CASE(8, 2) ZK_LEAVES_CASE(8, 3) ZK_LEAVES_CASE(8, 4)
+        ZK_LEAVES_CASE(9, 0) ZK_LEAVES_CASE(9, 1) ZK_LEAVES_CASE(9, 2) ZK_LEAVES_CASE(9, 3) ZK_LEAVES_CASE(9, 4)
+        ZK_LEAVES_CASE(10, 0) ZK_LEAVES_CASE(10, 1) ZK_LEAVES_CASE(10, 2) ZK_LEAVES_CASE(10, 3)
+        ZK_LEAVES_CASE(11, 0) ZK_LEAVES_CASE(11, 1) ZK_LEAVES_CASE(11, 2)
+        ZK_LEAVES_CASE(12, 0) ZK_LEAVES_CASE(12, 1)
+        default: return nullptr;
+    }
+}
+#undef ZK_LEAVES_CASE
+
 // out[rev(k) * B + b] = in[b * N + k] (zeknox kernels.cu:94-135).  A block
 // takes kTrK consecutive k of a chunk of up to kTrMaxPolys polynomials
 // (reads: kTrK contiguous words per polynomial) and writes each of the kTrK
@@ -460,6 +722,29 @@ size_t pass_smem(uint32_t l, uint32_t lg_t) {
 
 // after_pass: the previous launch on `s` is the pass before this one of the
 // same transform, so this pass may start while it drains (pdl.cuh).
+// ZK_NTT_GENERIC_PASSES=1 keeps the runtime-shaped pass kernels for every
+// shape (same outputs; for comparing the two forms).
+bool fixed_passes_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("ZK_NTT_GENERIC_PASSES");
+        return !(e && e[0] == '1');
+    }();
+    return on;
+}
+
+// The 160 KB dynamic shared memory attribute, once per (kernel, device).
+void set_smem_attr(PassKernel kern) {
+    static std::mutex mu;
+    static std::map<std::pair<PassKernel, int>, bool> done;
+    const int dev = current_device();
+    std::lock_guard<std::mutex> g(mu);
+    bool &d = done[{kern, dev}];
+    if (!d) {
+        ZK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        d = true;
+    }
+}
+
 // The transform's direction is a template parameter of the pass kernels (the
 // 8-point DFT's root multiplies differ), so each compiled kernel holds one form.
 void launch_pass(const PassArgs &a, uint64_t groups, cudaStream_t s, bool after_pass) {
@@ -472,7 +757,22 @@ void launch_pass(const PassArgs &a, uint64_t groups, cudaStream_t s, bool after_
         attr_set.fetch_or(1ull << dev);
     }
     require(groups < (1ull << 31), "transform too large for one launch");
-    auto kern = a.inverse ? ntt_pass_kernel<true> : ntt_pass_kernel<false>;
+    PassKernel kern = a.inverse ? ntt_pass_kernel<true> : ntt_pass_kernel<false>;
+    if (a.kind == 0 && a.tw_full && (a.pre_full || !a.pre_lo) && fixed_passes_enabled()) {
+        // the compile-time column pass, when this shape has one (lv as the kernel computes it)
+        const uint64_t S = 1ull << a.lg_s, L = 1ull << a.l;
+        uint32_t lv = a.l;
+        if (a.n_valid < (L << a.lg_s) && a.lg_pre == 0) {
+            const uint64_t nz = (a.n_valid + S - 1) >> a.lg_s;
+            lv = nz <= 1 ? 0 : 64 - __builtin_clzll(nz - 1);
+        }
+        PassKernel fixed = a.inverse ? column_fixed_kernel<true>(a.l, a.lg_t, lv)
+                                     : column_fixed_kernel<false>(a.l, a.lg_t, lv);
+        if (fixed) {
+            set_smem_attr(fixed);
+            kern = fixed;
+        }
+    }
     if (after_pass) {
         launch_after(kern, (unsigned)groups, kNttThreads, smem, s, a);
         return;
@@ -483,16 +783,12 @@ void launch_pass(const PassArgs &a, uint64_t groups, cudaStream_t s, bool after_
 
 void launch_leaves_pass(const PassArgs &a, uint64_t groups, cudaStream_t s) {
     const size_t smem = pass_smem(a.l, a.lg_t);
-    static std::atomic<uint64_t> attr_set{0};
-    const int dev = current_device();
-    if (dev < 64 && !(attr_set.load() & (1ull << dev))) {
-        ZK_CUDA(cudaFuncSetAttribute(ntt_last_pass_leaves<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     160 * 1024));
-        attr_set.fetch_or(1ull << dev);
-    }
+    PassKernel fixed = fixed_passes_enabled() ? leaves_fixed_kernel(a.l, a.lg_t) : nullptr;
+    PassKernel kern = fixed ? fixed : ntt_last_pass_leaves<false>;
+    set_smem_attr(kern);
     require(groups < (1ull << 31), "transform too large for one launch");
     require(!a.inverse, "the leaf layout is written by forward transforms only");
-    launch_after(ntt_last_pass_leaves<false>, (unsigned)groups, kNttThreads, smem, s, a);  // always after a pass
+    launch_after(kern, (unsigned)groups, kNttThreads, smem, s, a);  // always after a pass
 }
 
 }  // namespace
