@@ -542,6 +542,8 @@ PassKernel column_fixed_kernel(uint32_t l, uint32_t lg_t, uint32_t lv) {
     switch (l << 8 | lg_t << 4 | (l - lv)) {
         ZK_COLUMN_CASES(7, 5) ZK_COLUMN_CASES(8, 5) ZK_COLUMN_CASES(9, 4) ZK_COLUMN_CASES(10, 3)
         ZK_COLUMN_CASES(11, 2) ZK_COLUMN_CASES(12, 1)
+        ZK_COLUMN_CASES(7, 4) ZK_COLUMN_CASES(8, 4) ZK_COLUMN_CASES(9, 3) ZK_COLUMN_CASES(10, 2)
+        ZK_COLUMN_CASES(11, 1) ZK_COLUMN_CASES(12, 0)
         default: return nullptr;
     }
 #undef ZK_COLUMN_CASES
@@ -913,6 +915,13 @@ static void launch_plan(const NttJob &j, const PassArgs &base, const Plan &plan,
                 a.lg_pre = lg - a.l - lg_s;
                 a.lg_t = std::min<uint32_t>(ilog2_floor(kLinesElems) - a.l, lg_s);
                 a.lg_t = std::min<uint32_t>(a.lg_t, 5);
+                // With the one-load twiddle table (up to 2^20 points, the compile-time
+                // column kernels) half as many lines per block: half the shared
+                // memory, so more resident blocks hide the loads.  Measured, LDE to
+                // leaves: 135 x 2^15 -> 2^18 0.645 -> 0.625 ms, 64 x 2^17 -> 2^19
+                // 0.741 -> 0.676, 16 x 2^12 -> 2^15 0.026 -> 0.020; without the table
+                // (the generic pass) 300 x 2^19 -> 2^22 got slower (35.1 -> 36.7).
+                if (base.tw_full && a.lg_t > 0) a.lg_t--;
                 if (p == 0) {
                     a.src = j.src + b0 * j.src_stride;
                     a.src_poly_stride = j.src_stride;
