@@ -549,6 +549,71 @@ PassKernel column_fixed_kernel(uint32_t l, uint32_t lg_t, uint32_t lv) {
 #undef ZK_COLUMN_CASES
 }
 
+// The last pass of a multi-pass transform writing rows (kind 1 of
+// ntt_pass_kernel) with the line length (2^LG_L) and lines per block (2^LG_T)
+// fixed at compile time.  Line t of the block is prefix krev = c0 + t; its
+// element k has natural index c0 + t + Q k.  Thread t's elements are
+// t + 256 j, so the output column (t mod T) is fixed and k = t / T + j * 256 / T.
+template <int LG_L, int LG_T, bool INV>
+__global__ void __launch_bounds__(kNttThreads) ntt_rows_fixed(PassArgs a) {
+    constexpr uint32_t L = 1u << LG_L, T = 1u << LG_T, TP = T > 1 ? T + 1 : 1;
+    constexpr uint32_t PER = T * L / kNttThreads;  // elements per thread
+    static_assert(T * L % kNttThreads == 0 && T <= kNttThreads, "block elements: a multiple of the threads");
+    extern __shared__ uint64_t smem[];
+    uint64_t *tw = smem;
+    uint64_t *sm = smem + L;
+    for (uint32_t j = threadIdx.x; j < L; j += kNttThreads) tw[j] = __ldg(a.line_roots + (j << (kLineLgMax - LG_L)));
+    pdl_wait();  // the previous pass's output is read only from here on
+    const uint32_t lg_pre = a.lg_pre, lg_gpp = lg_pre - LG_T;  // groups per polynomial: 2^lg_gpp
+    const uint64_t g = blockIdx.x, poly0 = g >> lg_gpp, c0 = (g & ((1ull << lg_gpp) - 1)) << LG_T;
+    const uint64_t mask1 = (1ull << a.l_first) - 1;
+    const uint64_t *src = a.src + poly0 * a.src_poly_stride;
+#pragma unroll
+    for (uint32_t j = 0; j < PER; j++) {
+        uint32_t e, t;  // element t + 256 j: line position e of line t
+        if constexpr (LG_L >= 8) {
+            e = threadIdx.x + kNttThreads * (j & (L / kNttThreads - 1));
+            t = j / (L / kNttThreads);
+        } else {
+            e = threadIdx.x & (L - 1);
+            t = (threadIdx.x >> LG_L) + j * (kNttThreads >> LG_L);
+        }
+        const uint64_t krev = c0 + t;  // k_1 + N_1 k_2 (3 passes) or k_1 (2 passes)
+        const uint64_t kpos = ((krev & mask1) << (lg_pre - a.l_first)) | (krev >> a.l_first);
+        cp_async8(&sm[e * TP + t], src + (kpos << LG_L) + e);
+    }
+    cp_async_wait_all();
+    smem_dif_fixed<LG_L, LG_T, LG_L - 1, INV>(sm, tw);
+    constexpr uint32_t DK = kNttThreads >> LG_T;  // step of k between j and j + 1
+    const uint32_t t = threadIdx.x & (T - 1), kt = threadIdx.x >> LG_T;
+    const uint32_t krt = __brev(kt) >> (32 - LG_L);
+    const uint64_t o0 = c0 + t + ((uint64_t)kt << lg_pre);  // natural index of this thread's first element
+    uint64_t *dst = a.dst + poly0 * a.dst_poly_stride + o0;
+    const uint64_t *col = sm + t;
+#pragma unroll
+    for (uint32_t j = 0; j < PER; j++) {
+        const uint32_t kr = krt | brev_const(j * DK, LG_L);
+        const uint64_t step = (uint64_t)(j * DK) << lg_pre;
+        uint64_t v = col[kr * TP];
+        if (a.post_lo) v = nt_mul(v, pow_at(a.post_full, a.post_lo, a.post_hi, a.post_h, o0 + step));
+        if (a.scale != 1) v = nt_mul(v, a.scale);
+        dst[step] = v;
+    }
+}
+
+// The compiled (line length, lines per block) pairs of ntt_rows_fixed, per direction.
+template <bool INV>
+PassKernel rows_fixed_kernel(uint32_t l, uint32_t lg_t) {
+#define ZK_ROWS_CASE(LG_L, LG_T) \
+    case ((LG_L) << 4 | (LG_T)): return ntt_rows_fixed<LG_L, LG_T, INV>;
+    switch (l << 4 | lg_t) {
+        ZK_ROWS_CASE(6, 5) ZK_ROWS_CASE(7, 5) ZK_ROWS_CASE(8, 5) ZK_ROWS_CASE(9, 4) ZK_ROWS_CASE(10, 3)
+        ZK_ROWS_CASE(11, 2) ZK_ROWS_CASE(12, 1)
+        default: return nullptr;
+    }
+#undef ZK_ROWS_CASE
+}
+
 // ntt_last_pass_leaves with the line length (2^LG_L) and polynomials per
 // block (2^LG_P) fixed at compile time, for blocks whose P * L elements are a
 // multiple of the thread count: thread t's elements are t + 256 i, so their
@@ -734,16 +799,24 @@ bool fixed_passes_enabled() {
     return on;
 }
 
-// The 160 KB dynamic shared memory attribute, once per (kernel, device).
+// The 160 KB dynamic shared memory attribute, once per (kernel, device): a
+// fixed table (no host allocation on the launch path, which the
+// allocation-free LDE shares), one device bit mask per kernel.
 void set_smem_attr(PassKernel kern) {
+    constexpr int kSlots = 512;
     static std::mutex mu;
-    static std::map<std::pair<PassKernel, int>, bool> done;
+    static PassKernel keys[kSlots];
+    static uint64_t devs[kSlots];
     const int dev = current_device();
     std::lock_guard<std::mutex> g(mu);
-    bool &d = done[{kern, dev}];
-    if (!d) {
-        ZK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-        d = true;
+    int i = (int)(((uintptr_t)kern >> 4) % kSlots);
+    for (int n = 0; n < kSlots && keys[i] && keys[i] != kern; n++) i = (i + 1) % kSlots;
+    const bool known = keys[i] == kern && dev < 64 && (devs[i] >> dev & 1);
+    if (known) return;
+    ZK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    if (!keys[i] || keys[i] == kern) {  // remembered unless the table is full (then set on every launch)
+        keys[i] = kern;
+        if (dev < 64) devs[i] |= 1ull << dev;
     }
 }
 
@@ -770,6 +843,13 @@ void launch_pass(const PassArgs &a, uint64_t groups, cudaStream_t s, bool after_
         }
         PassKernel fixed = a.inverse ? column_fixed_kernel<true>(a.l, a.lg_t, lv)
                                      : column_fixed_kernel<false>(a.l, a.lg_t, lv);
+        if (fixed) {
+            set_smem_attr(fixed);
+            kern = fixed;
+        }
+    }
+    if (a.kind == 1 && fixed_passes_enabled()) {
+        PassKernel fixed = a.inverse ? rows_fixed_kernel<true>(a.l, a.lg_t) : rows_fixed_kernel<false>(a.l, a.lg_t);
         if (fixed) {
             set_smem_attr(fixed);
             kern = fixed;
