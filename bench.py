@@ -1023,7 +1023,7 @@ def served_section(args, zk, torch, baseline_legs: bool) -> dict:
 
     def served_run(arr):
         with zk.Server(hbm_budget_bytes=args.budget_gb << 30, slots=args.streams) as srv:
-            lat_s, caps_s, errs, tick = {}, {}, [], {}
+            lat_s, caps_s, errs, tick, split = {}, {}, [], {}, {}
 
             def client():  # completions in order; each tree released at once
                 try:
@@ -1032,6 +1032,7 @@ def served_section(args, zk, torch, baseline_legs: bool) -> dict:
                         if t is not None:
                             cap, lat = srv.wait(t)
                             lat_s[t], caps_s[t] = lat, cap
+                            split[t] = srv.job_times(t)
                             srv.release(t)
                 except Exception as e:  # noqa: BLE001 - reported by the main thread
                     errs.append(e)
@@ -1053,9 +1054,14 @@ def served_section(args, zk, torch, baseline_legs: bool) -> dict:
             st = srv.stats()
         lats = [lat_s[tick[j]] for j in range(n_jobs)]
         caps = [caps_s[tick[j]] for j in range(n_jobs)]
+        slow = sorted(range(n_jobs), key=lambda j: -lats[j])[: max(1, n_jobs // 100)]
         return {"p50_s": _pct(lats, 50), "p99_s": _pct(lats, 99), "elems_per_s": elems / span,
                 "started_ahead": st["ahead"], "max_queue": st["max_queue"],
-                "hbm_peak_gb": st["hbm_peak"] / 2**30, "clocks": clk.summary()}, caps
+                "hbm_peak_gb": st["hbm_peak"] / 2**30, "alloc_max_s": st["alloc_max_s"],
+                # the slowest 1 %: job, lg_n, polys, latency, seconds queued, seconds running
+                "slowest": [[j, jobs[j][0], jobs[j][1], round(lats[j], 4), *(round(x, 4) for x in split[tick[j]])]
+                            for j in slow],
+                "clocks": clk.summary()}, caps
 
     arrivals, res, caps_ref = None, None, None
     runs = {f: {"plain": [], "served": []} for f in args.served_rates}

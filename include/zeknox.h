@@ -258,6 +258,7 @@ typedef struct {
     double elems, elems_per_s;  /* committed LDE evaluations; first submit -> last completion */
     uint64_t hbm_in_use, hbm_peak;
     uint64_t ahead; /* jobs started ahead of an older queued job or beside a running one */
+    double alloc_max_s; /* longest host time one job's device allocations took */
 } ZkServerStats;
 ZK_EXTERN RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes, uint32_t n_slots, ZkServer **out);
 ZK_EXTERN RustError zk_server_submit(ZkServer *srv, const void *host_coeffs, uint32_t lg_n, uint32_t rate_bits,
@@ -275,6 +276,9 @@ ZK_EXTERN RustError zk_server_result(ZkServer *srv, uint64_t ticket, void **d_le
                                      void **d_cap);
 ZK_EXTERN RustError zk_server_release(ZkServer *srv, uint64_t ticket);
 ZK_EXTERN RustError zk_server_stats(ZkServer *srv, ZkServerStats *out);
+/* Where a completed job's latency went (before zk_server_release): submit ->
+ * start (queued_s) and start -> cap on the host (run_s). */
+ZK_EXTERN RustError zk_server_job_times(ZkServer *srv, uint64_t ticket, double *queued_s, double *run_s);
 /* Host-side fault injection for tests: the next n_jobs admitted jobs fail at
  * their at_allocation-th device allocation (1 = coefficients, 2 = leaves,
  * 3 = digests, ...) as if the pool were exhausted.  A failed job reports its

@@ -226,6 +226,14 @@ class Server:
         self._keep[t.value] = (None, cap_height)
         return t.value
 
+    def job_times(self, ticket: int):
+        """-> (seconds queued, seconds from start to the cap on the host) of a completed job."""
+        import ctypes
+
+        q, r = ctypes.c_double(), ctypes.c_double()
+        capi.check(capi.LIB.zk_server_job_times(self._h, ticket, ctypes.byref(q), ctypes.byref(r)))
+        return q.value, r.value
+
     def inject_failure(self, n_jobs: int, at_allocation: int):
         """Test hook: the next n_jobs admitted jobs fail at their at_allocation-th device allocation."""
         capi.check(capi.LIB.zk_server_inject_failure(self._h, n_jobs, at_allocation))

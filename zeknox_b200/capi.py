@@ -79,7 +79,8 @@ class ZkServerStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_uint64), ("queued", ctypes.c_uint64), ("max_queue", ctypes.c_uint64),
                 ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("max_s", ctypes.c_double),
                 ("elems", ctypes.c_double), ("elems_per_s", ctypes.c_double), ("hbm_in_use", ctypes.c_uint64),
-                ("hbm_peak", ctypes.c_uint64), ("ahead", ctypes.c_uint64)]
+                ("hbm_peak", ctypes.c_uint64), ("ahead", ctypes.c_uint64),
+                ("alloc_max_s", ctypes.c_double)]
 
 
 assert ctypes.sizeof(NTTConfig) == 24 and ctypes.sizeof(TransposeConfig) == 8
@@ -131,6 +132,7 @@ def _load() -> ctypes.CDLL:
         "zk_server_submit_seeded": (RustError, [vp, u64, u32, u32, u32, u32, u32, ctypes.POINTER(u64)]),
         "zk_server_inject_failure": (RustError, [vp, u32, u32]),
         "zk_fill_field_async": (RustError, [vp, u64, u64, vp]),
+        "zk_server_job_times": (RustError, [vp, u64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -294,6 +294,8 @@ struct ZkServer {
         std::vector<uint64_t> cap;  // the cap on the host, filled when the job completes
         int slot = -1;
         double est_s = 0;           // estimated GPU time alone
+        std::chrono::steady_clock::time_point t_admit{};  // when the dispatcher started it
+        double alloc_s = 0;         // host time its device allocations took
         double budget_s = 0;        // delay it may still take from later jobs started ahead of or beside it
         bool seeded = false;        // coefficients generated on the device from `seed`
         uint64_t seed = 0;
@@ -307,7 +309,16 @@ struct ZkServer {
     uint64_t budget = 0, in_use = 0, peak = 0;
     // Every job's delay budget: this fraction of its own estimated GPU time.
     double budget_frac = 0.05;
+    // The server's own memory pool (the budget is reserved in it) and an idle
+    // stream that released trees are freed on.  The pool never reuses a block
+    // by making the new job's stream wait for the stream that freed it (no
+    // internal dependencies): freed blocks are reused only once the free has
+    // executed.  A tree freed on its slot's stream, which may already run the
+    // next job, would otherwise tie a later job to that unrelated job.
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t free_stream = nullptr;
     uint64_t ahead = 0;  // jobs started ahead of an older queued job or beside a running one
+    double alloc_max_s = 0;  // longest time one job's device allocations took on the host
     // [slot][0]: high priority, [1]: normal priority, [2]: the slot's host-to-device copies
     std::vector<std::vector<cudaStream_t>> slots;
     // Per slot, pinned staging for the cap's device-to-host copy (grown by the
@@ -444,6 +455,7 @@ void ZkServer::run() {
         slot_busy[s] = true;
         J.slot = s;
         J.state = 1;
+        J.t_admit = std::chrono::steady_clock::now();
         running.push_back(t);
         n_running++;
         in_use += J.bytes + J.run_bytes;
@@ -476,13 +488,19 @@ void ZkServer::run() {
             auto alloc = [&](uint64_t **p, uint64_t bytes) {
                 if (++step == fail_at)
                     throw Error((int)cudaErrorMemoryAllocation, "injected allocation failure");
-                ZK_CUDA(cudaMallocAsync((void **)p, bytes, st));
+                ZK_CUDA(cudaMallocFromPoolAsync((void **)p, bytes, pool, st));
             };
+            const auto ta = std::chrono::steady_clock::now();
             alloc(&J.d_coeffs, sh.coeff_bytes());
             alloc(&J.d_leaves, sh.leaf_bytes());
             if (sh.n_digests()) alloc(&J.d_digests, sh.digest_bytes());
             alloc(&J.d_cap, sh.cap_bytes());
             if (sh.scratch_bytes()) alloc(&J.d_scratch, sh.scratch_bytes());
+            J.alloc_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - ta).count();
+            {
+                std::lock_guard<std::mutex> g(mu);
+                alloc_max_s = std::max(alloc_max_s, J.alloc_s);
+            }
             if (J.seeded) {
                 salt_run(J.d_coeffs, sh.n() * sh.batches, J.seed, st);  // the job's input, generated in place
                 commit_on(ctx, sh, J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch, st);
@@ -567,13 +585,25 @@ extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes,
             srv->slot_cap.push_back(staging);
             srv->slot_cap_bytes.push_back(64 << 10);
         }
-        // Reserve the budget in the pool (which keeps freed memory: its release
-        // threshold is unlimited), so admitted jobs are served from mapped
-        // memory.  If the device cannot hold it all now, jobs grow the pool.
+        ZK_CUDA(cudaStreamCreateWithFlags(&srv->free_stream, cudaStreamNonBlocking));
+        {
+            cudaMemPoolProps props{};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = device;
+            ZK_CUDA(cudaMemPoolCreate(&srv->pool, &props));
+            uint64_t thr = UINT64_MAX;  // keep freed memory mapped
+            ZK_CUDA(cudaMemPoolSetAttribute(srv->pool, cudaMemPoolAttrReleaseThreshold, &thr));
+            int no = 0, yes = 1;
+            ZK_CUDA(cudaMemPoolSetAttribute(srv->pool, cudaMemPoolReuseAllowInternalDependencies, &no));
+            ZK_CUDA(cudaMemPoolSetAttribute(srv->pool, cudaMemPoolReuseAllowOpportunistic, &yes));
+        }
+        // Reserve the budget in the pool, so admitted jobs are served from
+        // mapped memory.  If the device cannot hold it all now, jobs grow the pool.
         {
             cudaStream_t st = srv->slots[0][0];
             void *p = nullptr;
-            if (cudaMallocAsync(&p, hbm_budget_bytes, st) == cudaSuccess) {
+            if (cudaMallocFromPoolAsync(&p, hbm_budget_bytes, srv->pool, st) == cudaSuccess) {
                 ZK_CUDA(cudaFreeAsync(p, st));
                 ZK_CUDA(cudaStreamSynchronize(st));
             } else {
@@ -728,7 +758,9 @@ extern "C" RustError zk_server_release(ZkServer *srv, uint64_t ticket) {
         }
         ZK_CUDA(cudaSetDevice(srv->dev));
         if (J->state == 2) {
-            cudaStream_t st = J->stream;
+            // The job's work has completed (its completion callback ran), so the
+            // tree is freed on the idle stream, not behind whatever its slot runs now.
+            cudaStream_t st = srv->free_stream;
             if (J->d_leaves) ZK_CUDA(cudaFreeAsync(J->d_leaves, st));
             if (J->d_digests) ZK_CUDA(cudaFreeAsync(J->d_digests, st));
             if (J->d_cap) ZK_CUDA(cudaFreeAsync(J->d_cap, st));
@@ -759,6 +791,19 @@ extern "C" RustError zk_server_stats(ZkServer *srv, ZkServerStats *out) {
         out->hbm_in_use = srv->in_use;
         out->hbm_peak = srv->peak;
         out->ahead = srv->ahead;
+        out->alloc_max_s = srv->alloc_max_s;
+    });
+}
+
+extern "C" RustError zk_server_job_times(ZkServer *srv, uint64_t ticket, double *queued_s, double *run_s) {
+    return guard([&] {
+        require(srv != nullptr, "null server");
+        std::lock_guard<std::mutex> g(srv->mu);
+        auto it = srv->jobs.find(ticket);
+        require(it != srv->jobs.end() && it->second->state == 2, "ticket not completed");
+        const ZkServer::Job &J = *it->second;
+        if (queued_s) *queued_s = std::chrono::duration<double>(J.t_admit - J.t_submit).count();
+        if (run_s) *run_s = std::chrono::duration<double>(J.t_done - J.t_admit).count();
     });
 }
 
@@ -792,9 +837,15 @@ extern "C" RustError zk_server_destroy(ZkServer *srv) {
             for (cudaStream_t st : per) cudaStreamDestroy(st);
         for (uint64_t *p : srv->slot_cap)
             if (p) cudaFreeHost(p);
+        if (srv->free_stream) {
+            ZK_CUDA(cudaStreamSynchronize(srv->free_stream));
+            cudaStreamDestroy(srv->free_stream);
+        }
         // Hand the reserved budget back to the device.
-        cudaMemPool_t pool;
-        if (cudaDeviceGetDefaultMemPool(&pool, srv->dev) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+        if (srv->pool) {
+            cudaMemPoolTrimTo(srv->pool, 0);
+            cudaMemPoolDestroy(srv->pool);
+        }
     });
     delete srv;
     return r;
