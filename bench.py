@@ -1058,6 +1058,7 @@ def served_section(args, zk, torch, baseline_legs: bool) -> dict:
         return {"p50_s": _pct(lats, 50), "p99_s": _pct(lats, 99), "elems_per_s": elems / span,
                 "started_ahead": st["ahead"], "max_queue": st["max_queue"],
                 "hbm_peak_gb": st["hbm_peak"] / 2**30, "alloc_max_s": st["alloc_max_s"],
+                "pool_gb": [st["pool_reserved_start"] / 2**30, st["pool_reserved_high"] / 2**30],
                 # the slowest 1 %: job, lg_n, polys, latency, seconds queued, seconds running
                 "slowest": [[j, jobs[j][0], jobs[j][1], round(lats[j], 4), *(round(x, 4) for x in split[tick[j]])]
                             for j in slow],

@@ -259,6 +259,8 @@ typedef struct {
     uint64_t hbm_in_use, hbm_peak;
     uint64_t ahead; /* jobs started ahead of an older queued job or beside a running one */
     double alloc_max_s; /* longest host time one job's device allocations took */
+    uint64_t pool_reserved_start; /* bytes the server's memory pool mapped at creation */
+    uint64_t pool_reserved_high;  /* most bytes it has mapped since (above the first: it grew) */
 } ZkServerStats;
 ZK_EXTERN RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes, uint32_t n_slots, ZkServer **out);
 ZK_EXTERN RustError zk_server_submit(ZkServer *srv, const void *host_coeffs, uint32_t lg_n, uint32_t rate_bits,

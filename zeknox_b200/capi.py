@@ -80,7 +80,8 @@ class ZkServerStats(ctypes.Structure):
                 ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("max_s", ctypes.c_double),
                 ("elems", ctypes.c_double), ("elems_per_s", ctypes.c_double), ("hbm_in_use", ctypes.c_uint64),
                 ("hbm_peak", ctypes.c_uint64), ("ahead", ctypes.c_uint64),
-                ("alloc_max_s", ctypes.c_double)]
+                ("alloc_max_s", ctypes.c_double), ("pool_reserved_start", ctypes.c_uint64),
+                ("pool_reserved_high", ctypes.c_uint64)]
 
 
 assert ctypes.sizeof(NTTConfig) == 24 and ctypes.sizeof(TransposeConfig) == 8

@@ -317,6 +317,7 @@ struct ZkServer {
     // next job, would otherwise tie a later job to that unrelated job.
     cudaMemPool_t pool = nullptr;
     cudaStream_t free_stream = nullptr;
+    uint64_t reserved_start = 0;  // bytes the pool had mapped when the server started
     uint64_t ahead = 0;  // jobs started ahead of an older queued job or beside a running one
     double alloc_max_s = 0;  // longest time one job's device allocations took on the host
     // [slot][0]: high priority, [1]: normal priority, [2]: the slot's host-to-device copies
@@ -598,17 +599,27 @@ extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes,
             ZK_CUDA(cudaMemPoolSetAttribute(srv->pool, cudaMemPoolReuseAllowInternalDependencies, &no));
             ZK_CUDA(cudaMemPoolSetAttribute(srv->pool, cudaMemPoolReuseAllowOpportunistic, &yes));
         }
-        // Reserve the budget in the pool, so admitted jobs are served from
-        // mapped memory.  If the device cannot hold it all now, jobs grow the pool.
+        // Reserve the budget in the pool, with an eighth more for fragmentation,
+        // so admitted jobs are served from mapped memory: growing the pool while
+        // jobs run maps physical memory on the dispatcher thread (about a second
+        // for tens of GB), which stalls every admission meanwhile.  Memory that
+        // the device's default pool keeps cached from earlier calls is handed
+        // back first.  If the device cannot hold the reservation, the budget
+        // alone is tried, then none (jobs grow the pool).
         {
+            cudaMemPool_t def;
+            if (cudaDeviceGetDefaultMemPool(&def, device) == cudaSuccess) cudaMemPoolTrimTo(def, 0);
             cudaStream_t st = srv->slots[0][0];
-            void *p = nullptr;
-            if (cudaMallocFromPoolAsync(&p, hbm_budget_bytes, srv->pool, st) == cudaSuccess) {
-                ZK_CUDA(cudaFreeAsync(p, st));
-                ZK_CUDA(cudaStreamSynchronize(st));
-            } else {
+            for (uint64_t want : {hbm_budget_bytes + hbm_budget_bytes / 8, hbm_budget_bytes}) {
+                void *p = nullptr;
+                if (cudaMallocFromPoolAsync(&p, want, srv->pool, st) == cudaSuccess) {
+                    ZK_CUDA(cudaFreeAsync(p, st));
+                    ZK_CUDA(cudaStreamSynchronize(st));
+                    break;
+                }
                 cudaGetLastError();
             }
+            cudaMemPoolGetAttribute(srv->pool, cudaMemPoolAttrReservedMemCurrent, &srv->reserved_start);
         }
         ZkServer *p = srv.get();
         srv->dispatcher = std::thread([p] {
@@ -792,6 +803,8 @@ extern "C" RustError zk_server_stats(ZkServer *srv, ZkServerStats *out) {
         out->hbm_peak = srv->peak;
         out->ahead = srv->ahead;
         out->alloc_max_s = srv->alloc_max_s;
+        out->pool_reserved_start = srv->reserved_start;
+        if (srv->pool) cudaMemPoolGetAttribute(srv->pool, cudaMemPoolAttrReservedMemHigh, &out->pool_reserved_high);
     });
 }
 
