@@ -189,7 +189,7 @@ def test_init_coset_other_generator(zk, oracle):
 
 
 @pytest.mark.parametrize("lg,batches", [(0, 1), (1, 3), (5, 7), (10, 135), (13, 16), (18, 135), (6, 1000), (4, 200),
-                                        (7, 193)])
+                                        (7, 193), (7, 1), (8, 2), (9, 385), (11, 64)])
 def test_transpose_rev(zk, oracle, lg, batches):
     x = oracle.field_elems(9 + lg, batches << lg)
     out = np.zeros_like(x)
@@ -201,6 +201,21 @@ def test_transpose_rev(zk, oracle, lg, batches):
     c.are_inputs_on_device = c.are_outputs_on_device = True
     zk.transpose_rev_batch(0, d_out.data_ptr(), d_in.data_ptr(), lg, c)
     assert np.array_equal(_host(d_out), out)
+
+
+@pytest.mark.parametrize("lg,batches", [(12, 135), (7, 3)])
+def test_transpose_rev_input_only_8_byte_aligned(zk, oracle, lg, batches):
+    """A device input 8 bytes past a 16-byte boundary takes the 8-byte-load
+    form of the transpose; the output must not change."""
+    x = oracle.field_elems(31 + lg, batches << lg)
+    c = zk.TransposeConfig.default()
+    c.batches = batches
+    c.are_inputs_on_device = c.are_outputs_on_device = True
+    d_in = _dev(np.concatenate([np.zeros(1, dtype=np.uint64), x]))
+    assert (d_in.data_ptr() + 8) % 16 == 8
+    d_out = _dev(np.zeros_like(x))
+    zk.transpose_rev_batch(0, d_out.data_ptr(), d_in.data_ptr() + 8, lg, c)
+    assert np.array_equal(_host(d_out), oracle.transpose_rev(x, lg, batches))
 
 
 def test_lde_multi_gpu_entry(zk, oracle):

@@ -91,6 +91,11 @@ def nt_add(a, b):
     return mad_wide(m, M32, (s1 << 32) | s0)
 
 
+def nt_add_neg(a, b):
+    """nt_add as compiled: a - (p - b) through nt_sub (p - b may be p itself)."""
+    return nt_sub(a, P - b)
+
+
 def nt_canon(x):
     f = Flags()
     x0, x1 = halves(x)
@@ -137,6 +142,7 @@ def test_edge_operands():
             a, b = e1 % P, e2 % P
             assert nt_sub(a, b) == (a - b) % P
             assert nt_add(a, b) == (a + b) % P
+            assert nt_add_neg(a, b) == (a + b) % P
             assert nt_mul(a, b) == (a * b) % P
 
 
@@ -147,6 +153,7 @@ def test_random_operands(seed):
         a, b = rng.randrange(P), rng.randrange(P)
         assert nt_sub(a, b) == (a - b) % P
         assert nt_add(a, b) == (a + b) % P
+        assert nt_add_neg(a, b) == (a + b) % P
         assert nt_mul(a, b) == (a * b) % P
         x = rng.choice([rng.randrange(2**64), P + rng.randrange(2**32 - 1), rng.randrange(P)])
         assert nt_canon(x) == x % P

@@ -58,8 +58,15 @@ __device__ __forceinline__ uint64_t nt_sub(uint64_t a, uint64_t b) {
     return ((uint64_t)hi << 32) | lo;
 }
 
-// a + b mod p for canonical a, b: s = a + b mod 2^64 takes + (2^32 - 1) when the
-// sum carried out of 2^64 or s >= p (at most one of the two happens).
+// a + b mod p for canonical a, b, as a - (p - b): p - b is in (0, p], and
+// nt_sub is exact for a subtrahend of p too (a - p borrows, and the
+// correction adds p back), so the sum costs a 64-bit negation and the
+// three-instruction subtraction instead of two carry chains and a fold.
+#ifndef ZK_NT_ADD_CARRY
+__device__ __forceinline__ uint64_t nt_add(uint64_t a, uint64_t b) { return nt_sub(a, ZK_P - b); }
+#else
+// s = a + b mod 2^64 takes + (2^32 - 1) when the sum carried out of 2^64 or
+// s >= p (at most one of the two happens).
 __device__ __forceinline__ uint64_t nt_add(uint64_t a, uint64_t b) {
     uint32_t s0, s1, m;
     asm("{\n\t"
@@ -75,6 +82,7 @@ __device__ __forceinline__ uint64_t nt_add(uint64_t a, uint64_t b) {
         : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)), "r"(kLo32));
     return fold_k(m, ((uint64_t)s1 << 32) | s0);
 }
+#endif
 
 // (h1, h0, l1, l0) 128-bit -> u64 congruent mod p (not canonical):
 // l - h1 (minus 2^32 - 1 on a borrow, as in nt_sub), then + h0 (2^32 - 1)

@@ -10,8 +10,9 @@
 //
 // ZkServer: a request loop for commits that arrive over time.  A dispatcher
 // thread admits queued jobs onto free slots while their device memory fits an
-// HBM budget (reserved in the device's memory pool when the server starts, so
-// an admitted job never waits for physical memory); admitted jobs run
+// HBM budget (reserved in the server's memory pool when it starts, so an
+// admitted job rarely waits for physical memory); each slot's worker thread
+// allocates and launches the jobs admitted to it, and admitted jobs run
 // concurrently.  Admission is first in, first out, with one exception that
 // is bounded per job: every job carries a delay budget, a fraction of its own
 // estimated GPU time alone (est, from its size).  A job may start ahead of
@@ -296,6 +297,7 @@ struct ZkServer {
         double est_s = 0;           // estimated GPU time alone
         std::chrono::steady_clock::time_point t_admit{};  // when the dispatcher started it
         double alloc_s = 0;         // host time its device allocations took
+        uint32_t fail_at = 0;       // injected failure: the 1-based allocation made to fail (0: none)
         double budget_s = 0;        // delay it may still take from later jobs started ahead of or beside it
         bool seeded = false;        // coefficients generated on the device from `seed`
         uint64_t seed = 0;
@@ -332,6 +334,9 @@ struct ZkServer {
     std::vector<uint64_t> running;     // tickets of admitted, unfinished jobs
     std::mutex mu;
     std::condition_variable cv;        // dispatcher wake-up
+    std::condition_variable work_cv;   // slot workers' wake-up
+    std::vector<uint64_t> slot_job;    // per slot: the ticket handed to its worker (0: none)
+    std::vector<std::thread> workers;  // one per slot
     std::condition_variable done_cv;   // completions
     std::deque<uint64_t> queue;
     std::deque<uint64_t> done_q;       // completed or failed, not yet returned by wait_any
@@ -351,6 +356,8 @@ struct ZkServer {
     uint32_t inject_jobs = 0, inject_step = 0;
 
     void run();
+    void work(int s);
+    void start(Job &J, DeviceCtx &ctx);
     void fail_admitted(Job &J, const char *why);
     uint64_t submit(std::unique_ptr<Job> J);
 };
@@ -387,8 +394,6 @@ void CUDART_CB on_done(void *p) {
 }  // namespace
 
 void ZkServer::run() {
-    ZK_CUDA(cudaSetDevice(dev));
-    DeviceCtx &ctx = device_ctx(dev);
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
         cv.wait(lk, [&] {
@@ -461,72 +466,90 @@ void ZkServer::run() {
         n_running++;
         in_use += J.bytes + J.run_bytes;
         peak = std::max(peak, in_use);
-        uint32_t fail_at = 0;  // 1-based allocation that is made to fail (0: none)
         if (inject_jobs) {
             inject_jobs--;
-            fail_at = inject_step;
+            J.fail_at = inject_step;
         }
+        // The slot's worker allocates and launches, so that an allocation
+        // which blocks on the host (the pool waiting for outstanding frees when
+        // its free memory is fragmented; measured up to ~2 s for an 80 GB tree)
+        // delays only this job, not the admission of every job behind it.
+        slot_job[s] = t;
+        work_cv.notify_all();
+    }
+}
+
+// Slot s's worker: starts each job the dispatcher hands to the slot.
+void ZkServer::work(int s) {
+    ZK_CUDA(cudaSetDevice(dev));
+    DeviceCtx &ctx = device_ctx(dev);
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+        work_cv.wait(lk, [&] { return stop || slot_job[s] != 0; });
+        if (stop) return;  // a job handed over but not started is dropped with the server
+        Job &J = *jobs[slot_job[s]];
+        slot_job[s] = 0;
         lk.unlock();
-        try {
-            // priority by size: < 20 ms of estimated GPU time high, everything else normal.  (A third,
-            // lowest level for the large jobs measured worse: 80 jobs at 0.75x load, p99 2.66 s and
-            // throughput 0.95x FIFO, against 2.11 s and 0.99x with two levels.)
-            cudaStream_t st = slots[s][J.est_s < 0.02 ? 0 : 1];
-            J.stream = st;
-            const Shape &sh = J.sh;
-            if (slot_cap_bytes[s] < sh.cap_bytes()) {
-                // Rare (a larger cap than this slot has staged so far), and done
-                // without the lock: pinned allocation may synchronise with the
-                // device, whose completion callbacks take the lock.  The slot is
-                // this job's, and its previous job's callback has run.
-                if (slot_cap[s]) cudaFreeHost(slot_cap[s]);
-                slot_cap[s] = nullptr;
-                slot_cap_bytes[s] = 0;
-                ZK_CUDA(cudaMallocHost((void **)&slot_cap[s], sh.cap_bytes()));
-                slot_cap_bytes[s] = sh.cap_bytes();
-            }
-            uint32_t step = 0;
-            auto alloc = [&](uint64_t **p, uint64_t bytes) {
-                if (++step == fail_at)
-                    throw Error((int)cudaErrorMemoryAllocation, "injected allocation failure");
-                ZK_CUDA(cudaMallocFromPoolAsync((void **)p, bytes, pool, st));
-            };
-            const auto ta = std::chrono::steady_clock::now();
-            alloc(&J.d_coeffs, sh.coeff_bytes());
-            alloc(&J.d_leaves, sh.leaf_bytes());
-            if (sh.n_digests()) alloc(&J.d_digests, sh.digest_bytes());
-            alloc(&J.d_cap, sh.cap_bytes());
-            if (sh.scratch_bytes()) alloc(&J.d_scratch, sh.scratch_bytes());
-            J.alloc_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - ta).count();
-            {
-                std::lock_guard<std::mutex> g(mu);
-                alloc_max_s = std::max(alloc_max_s, J.alloc_s);
-            }
-            if (J.seeded) {
-                salt_run(J.d_coeffs, sh.n() * sh.batches, J.seed, st);  // the job's input, generated in place
-                commit_on(ctx, sh, J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch, st);
-            } else {
-                commit_from_host(ctx, sh, J.host_coeffs, J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch,
-                                 st, slots[s][2]);
-            }
-            ZK_CUDA(cudaMemcpyAsync(slot_cap[s], J.d_cap, sh.cap_bytes(), cudaMemcpyDeviceToHost, st));
-            ZK_CUDA(cudaFreeAsync(J.d_coeffs, st));
-            J.d_coeffs = nullptr;
-            if (J.d_scratch) ZK_CUDA(cudaFreeAsync(J.d_scratch, st));
-            J.d_scratch = nullptr;
-            ZK_CUDA(cudaLaunchHostFunc(st, on_done, new DoneCtx{this, t}));
-        } catch (const Error &e) {
-            J.err = e.code;
-            fail_admitted(J, e.what());
-            lk.lock();
-            continue;
-        } catch (const std::exception &e) {
-            J.err = -(int)cudaErrorUnknown;
-            fail_admitted(J, e.what());
-            lk.lock();
-            continue;
-        }
+        start(J, ctx);
         lk.lock();
+    }
+}
+
+// Allocate a job's buffers from the pool and launch it on its slot's streams
+// (called without `mu` held); a failure releases what it took (fail_admitted).
+void ZkServer::start(Job &J, DeviceCtx &ctx) {
+    const int s = J.slot;
+    try {
+        // priority by size: < 20 ms of estimated GPU time high, everything else normal.  (A third,
+        // lowest level for the large jobs measured worse: 80 jobs at 0.75x load, p99 2.66 s and
+        // throughput 0.95x FIFO, against 2.11 s and 0.99x with two levels.)
+        cudaStream_t st = slots[s][J.est_s < 0.02 ? 0 : 1];
+        J.stream = st;
+        const Shape &sh = J.sh;
+        if (slot_cap_bytes[s] < sh.cap_bytes()) {
+            // Rare (a larger cap than this slot has staged so far).  The slot is
+            // this job's, and its previous job's completion callback has run.
+            if (slot_cap[s]) cudaFreeHost(slot_cap[s]);
+            slot_cap[s] = nullptr;
+            slot_cap_bytes[s] = 0;
+            ZK_CUDA(cudaMallocHost((void **)&slot_cap[s], sh.cap_bytes()));
+            slot_cap_bytes[s] = sh.cap_bytes();
+        }
+        uint32_t step = 0;
+        auto alloc = [&](uint64_t **p, uint64_t bytes) {
+            if (++step == J.fail_at) throw Error((int)cudaErrorMemoryAllocation, "injected allocation failure");
+            ZK_CUDA(cudaMallocFromPoolAsync((void **)p, bytes, pool, st));
+        };
+        const auto ta = std::chrono::steady_clock::now();
+        alloc(&J.d_coeffs, sh.coeff_bytes());
+        alloc(&J.d_leaves, sh.leaf_bytes());
+        if (sh.n_digests()) alloc(&J.d_digests, sh.digest_bytes());
+        alloc(&J.d_cap, sh.cap_bytes());
+        if (sh.scratch_bytes()) alloc(&J.d_scratch, sh.scratch_bytes());
+        J.alloc_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - ta).count();
+        {
+            std::lock_guard<std::mutex> g(mu);
+            alloc_max_s = std::max(alloc_max_s, J.alloc_s);
+        }
+        if (J.seeded) {
+            salt_run(J.d_coeffs, sh.n() * sh.batches, J.seed, st);  // the job's input, generated in place
+            commit_on(ctx, sh, J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch, st);
+        } else {
+            commit_from_host(ctx, sh, J.host_coeffs, J.d_coeffs, J.d_leaves, J.d_digests, J.d_cap, J.d_scratch,
+                             st, slots[s][2]);
+        }
+        ZK_CUDA(cudaMemcpyAsync(slot_cap[s], J.d_cap, sh.cap_bytes(), cudaMemcpyDeviceToHost, st));
+        ZK_CUDA(cudaFreeAsync(J.d_coeffs, st));
+        J.d_coeffs = nullptr;
+        if (J.d_scratch) ZK_CUDA(cudaFreeAsync(J.d_scratch, st));
+        J.d_scratch = nullptr;
+        ZK_CUDA(cudaLaunchHostFunc(st, on_done, new DoneCtx{this, J.ticket}));
+    } catch (const Error &e) {
+        J.err = e.code;
+        fail_admitted(J, e.what());
+    } catch (const std::exception &e) {
+        J.err = -(int)cudaErrorUnknown;
+        fail_admitted(J, e.what());
     }
 }
 
@@ -581,6 +604,7 @@ extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes,
             per.push_back(cs);
             srv->slots.push_back(per);
             srv->slot_busy.push_back(false);
+            srv->slot_job.push_back(0);
             uint64_t *staging = nullptr;
             ZK_CUDA(cudaMallocHost((void **)&staging, 64 << 10));  // caps of up to 2^11 digests
             srv->slot_cap.push_back(staging);
@@ -622,15 +646,18 @@ extern "C" RustError zk_server_create(int32_t device, uint64_t hbm_budget_bytes,
             cudaMemPoolGetAttribute(srv->pool, cudaMemPoolAttrReservedMemCurrent, &srv->reserved_start);
         }
         ZkServer *p = srv.get();
-        srv->dispatcher = std::thread([p] {
+        auto guarded = [p](auto body) {
             try {
-                p->run();
+                body();
             } catch (const std::exception &e) {
                 std::lock_guard<std::mutex> g(p->mu);
                 p->fatal = e.what();
                 p->done_cv.notify_all();
             }
-        });
+        };
+        srv->dispatcher = std::thread([p, guarded] { guarded([p] { p->run(); }); });
+        for (uint32_t i = 0; i < n_slots; i++)
+            srv->workers.emplace_back([p, guarded, i] { guarded([p, i] { p->work((int)i); }); });
         *out = srv.release();
     });
 }
@@ -835,8 +862,11 @@ extern "C" RustError zk_server_destroy(ZkServer *srv) {
         std::lock_guard<std::mutex> g(srv->mu);
         srv->stop = true;
         srv->cv.notify_all();
+        srv->work_cv.notify_all();
     }
     if (srv->dispatcher.joinable()) srv->dispatcher.join();
+    for (std::thread &w : srv->workers)
+        if (w.joinable()) w.join();
     RustError r = guard([&] {
         ZK_CUDA(cudaSetDevice(srv->dev));
         for (auto &per : srv->slots)
