@@ -74,6 +74,61 @@ def profile_figures() -> dict:
     return d
 
 
+FIGURES_COMMAND = ('ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum,'
+                   'smsp__inst_executed.sum --clock-control none -k regex:"merkle_|ntt_|transpose" -c 60 --csv '
+                   '--log-file figures.csv python bench.py --steps 2 --warmup 3 --no-cpu-baseline --sections none')
+
+
+def write_profile_figures(csv_path, out=None) -> dict:
+    """profiles/ncu_figures.json from the CSV launch list of FIGURES_COMMAND:
+    the launches of one fused step (the first LDE pass up to the next LDE pass
+    after the Merkle kernels) and the plain path's transpose, per launch, stamped
+    with the hash of the current kernel sources."""
+    import collections
+    import csv
+
+    per = collections.OrderedDict()
+    hdr = None
+    with open(csv_path) as f:
+        for r in csv.reader(f):
+            if len(r) > 5 and r[0] == "ID":
+                hdr = r
+                continue
+            if hdr and len(r) == len(hdr):
+                d = dict(zip(hdr, r))
+                e = per.setdefault(int(d["ID"]), {"name": d["Kernel Name"]})
+                e[d["Metric Name"]] = float(d["Metric Value"].replace(",", ""))
+    launches = list(per.values())
+    i = next(i for i, k in enumerate(launches) if "ntt_" in k["name"])
+    step = []
+    while i < len(launches):
+        step.append(launches[i])
+        i += 1
+        if i < len(launches) and "ntt_" in launches[i]["name"] and any("merkle" in k["name"] for k in step):
+            break
+    lde = [k for k in step if "ntt_" in k["name"]]
+    mk = [k for k in step if "merkle" in k["name"]]
+    tr = [k for k in launches if "transpose" in k["name"]]
+    b, n_pts = 135, 1 << 18
+    perms = n_pts * 17 + 16 * ((n_pts >> 4) - 2) + 16  # leaf sponges of 135 words, inner nodes, cap 4
+    dram = lambda ks: sum(k["dram__bytes_read.sum"] + k["dram__bytes_write.sum"] for k in ks)  # noqa: E731
+    inst = lambda ks: sum(k["smsp__inst_executed.sum"] for k in ks)  # noqa: E731
+    names = lambda ks: [k["name"].split("(")[0][-60:] for k in ks]  # noqa: E731
+    fig = {"sources_sha256": kernel_sources_sha256(),
+           "command": FIGURES_COMMAND + "; then python bench.py --figures-from figures.csv",
+           "kernels": {
+               f"merkle poseidon {n_pts}x{b} cap 4": {
+                   "dram_bytes_per_launch": dram(mk), "thread_inst_per_perm": inst(mk) * 32 / perms,
+                   "launches": names(mk)},
+               f"lde_leaves {b}x2^15 rate 3": {
+                   "dram_bytes_per_launch": dram(lde), "thread_inst_per_elem": inst(lde) * 32 / (b * n_pts),
+                   "launches": names(lde)}}}
+    if tr:
+        fig["kernels"][f"transpose_rev {b}x2^18"] = {"dram_bytes_per_launch": dram(tr[:1]), "launches": names(tr[:1])}
+    Path(out or PROFILE_FIGURES).write_text(json.dumps(fig, indent=1) + "\n")
+    return fig
+
+
 def job_seed(config: int, j: int) -> int:
     """Seed of job j of a multi-job configuration: (0x5EED0000 + config) xor SplitMix64's output for j."""
     z = ((j + 1) * 0x9E3779B97F4A7C15) & (2**64 - 1)
@@ -302,7 +357,12 @@ def main() -> None:
     ap.add_argument("--served-replay", action="store_true",
                     help="time the plain FIFO arm by a real-time replay at each rate")
     ap.add_argument("--oracle-sample", type=int, default=6, help="jobs per section recomputed on the host")
+    ap.add_argument("--figures-from", metavar="CSV",
+                    help="write profiles/ncu_figures.json from the launch list of FIGURES_COMMAND, then exit")
     args = ap.parse_args()
+    if args.figures_from:
+        print(json.dumps(write_profile_figures(args.figures_from)["kernels"]))
+        return
     if args.workload != "commit" and args.impl == "ours":
         {"merkle": run_merkle_only, "sweep": run_sweep, "batched": run_batched, "served": run_served,
          "fri": run_fri, "field-ops": run_field_ops, "tensor-bound": run_tensor_bound}[args.workload](args)

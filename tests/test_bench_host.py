@@ -70,3 +70,33 @@ def test_profile_figures_only_for_the_sources_they_were_captured_from(tmp_path, 
     f.write_text(json.dumps({"sources_sha256": bench.kernel_sources_sha256(),
                              "kernels": {"k": {"dram_bytes_per_launch": 1}}}))
     assert bench.profile_figures()["kernels"]["k"]["dram_bytes_per_launch"] == 1
+
+
+def test_profile_figures_written_from_a_launch_list(tmp_path):
+    """The figures file is derived from ncu's CSV launch list of one fused step
+    (LDE passes, then the Merkle kernels) plus the plain path's transpose."""
+    import csv
+
+    import bench
+
+    cols = ["ID", "Process ID", "Process Name", "Host Name", "Kernel Name", "Context", "Stream", "Block Size",
+            "Grid Size", "Device", "CC", "Section Name", "Metric Name", "Metric Unit", "Metric Value"]
+    launches = ["ntt_column_fixed<9, 3, 6, 0>(PassArgs)", "ntt_leaves_fixed<9, 3>(PassArgs)",
+                "merkle_leaves_hex(...)", "merkle_level(...)", "ntt_column_fixed<9, 3, 6, 0>(PassArgs)",
+                "transpose_rev_kernel<true>(...)"]
+    path = tmp_path / "figures.csv"
+    with open(path, "w", newline="") as f:
+        w = csv.writer(f)
+        w.writerow(cols)
+        for i, name in enumerate(launches):
+            for m, v in [("dram__bytes_read.sum", 1000 * (i + 1)), ("dram__bytes_write.sum", 10),
+                         ("smsp__inst_executed.sum", 2 ** 20), ("gpu__time_duration.sum", 5)]:
+                w.writerow([i, 1, "python", "h", name, 1, 7, "(256, 1, 1)", "(8, 1, 1)", 0, "10.0", "", m, "", f"{v:,}"])
+    out = tmp_path / "fig.json"
+    fig = bench.write_profile_figures(path, out)
+    k = fig["kernels"]
+    assert k["lde_leaves 135x2^15 rate 3"]["dram_bytes_per_launch"] == 1010 + 2010
+    assert k["merkle poseidon 262144x135 cap 4"]["dram_bytes_per_launch"] == 3010 + 4010
+    assert k["transpose_rev 135x2^18"]["dram_bytes_per_launch"] == 6010
+    assert abs(k["lde_leaves 135x2^15 rate 3"]["thread_inst_per_elem"] - 2 * 2 ** 20 * 32 / (135 << 18)) < 1e-9
+    assert json.loads(out.read_text())["sources_sha256"] == bench.kernel_sources_sha256()

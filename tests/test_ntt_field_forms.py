@@ -1,5 +1,5 @@
-"""Field operations written as PTX carry sequences: the NTT's nt_sub, nt_add,
-nt_canon, nt_reduce128 and the x 2^24 fold of gl_mul2_24 (ntt_field.cuh), and
+"""Field operations written as PTX carry sequences: the NTT's nt_sub, nt_add
+(a subtraction of the negation), nt_canon, nt_reduce128 and the x 2^24 fold of gl_mul2_24 (ntt_field.cuh), and
 the hash S-box's sqr_wide (gl64.cuh).  Each is replayed here instruction by
 instruction with PTX's CC.CF semantics (add.cc / addc carry, sub.cc / subc
 borrow, mad.lo.cc / madc.hi.cc, shf.l.wrap) and checked exactly against the
@@ -79,20 +79,7 @@ def nt_sub(a, b):
 
 
 def nt_add(a, b):
-    f = Flags()
-    a0, a1 = halves(a)
-    b0, b1 = halves(b)
-    s0 = f.add_cc(a0, b0)
-    s1 = f.addc_cc(a1, b1)
-    c0 = f.addc(0, 0)
-    f.add_cc(s0, M32)
-    f.addc_cc(s1, 0)
-    m = f.addc(c0, 0)
-    return mad_wide(m, M32, (s1 << 32) | s0)
-
-
-def nt_add_neg(a, b):
-    """nt_add as compiled: a - (p - b) through nt_sub (p - b may be p itself)."""
+    """nt_add: a - (p - b) through nt_sub (p - b is p itself when b = 0)."""
     return nt_sub(a, P - b)
 
 
@@ -142,7 +129,6 @@ def test_edge_operands():
             a, b = e1 % P, e2 % P
             assert nt_sub(a, b) == (a - b) % P
             assert nt_add(a, b) == (a + b) % P
-            assert nt_add_neg(a, b) == (a + b) % P
             assert nt_mul(a, b) == (a * b) % P
 
 
@@ -153,7 +139,6 @@ def test_random_operands(seed):
         a, b = rng.randrange(P), rng.randrange(P)
         assert nt_sub(a, b) == (a - b) % P
         assert nt_add(a, b) == (a + b) % P
-        assert nt_add_neg(a, b) == (a + b) % P
         assert nt_mul(a, b) == (a * b) % P
         x = rng.choice([rng.randrange(2**64), P + rng.randrange(2**32 - 1), rng.randrange(P)])
         assert nt_canon(x) == x % P

@@ -631,13 +631,21 @@ __global__ void __launch_bounds__(kNttThreads) ntt_leaves_fixed(PassArgs a) {
     for (uint32_t j = threadIdx.x; j < L; j += kNttThreads) tw[j] = __ldg(a.line_roots + (j << (kLineLgMax - LG_L)));
     pdl_wait();  // the previous pass's output is read only from here on
     const uint32_t lg_pre = a.lg_pre;
-#ifdef ZK_LEAVES_GROUP_FAST
-    // consecutive blocks: the polynomial groups of one set of leaf rows
+    // With 16 or more polynomial groups (leaf rows of at least 16 runs written
+    // by different blocks), consecutive blocks take the groups of one set of
+    // leaf rows, so each row's sectors are completed while they are in L2
+    // (135 x 2^15 -> 2^18, 17 groups: 0.613 -> 0.604 ms); with fewer groups,
+    // consecutive blocks take consecutive rows of one group (that order
+    // measured 0.3-4 % faster there).
     const uint32_t ngroups = (uint32_t)((a.batches + P - 1) >> LG_P);
-    const uint64_t krev = blockIdx.x / ngroups, p0 = (uint64_t)(blockIdx.x - krev * ngroups) << LG_P;
-#else
-    const uint64_t krev = blockIdx.x & ((1ull << lg_pre) - 1), p0 = (uint64_t)(blockIdx.x >> lg_pre) << LG_P;
-#endif
+    uint64_t krev, p0;
+    if (ngroups >= 16) {
+        krev = blockIdx.x / ngroups;
+        p0 = (uint64_t)(blockIdx.x - krev * ngroups) << LG_P;
+    } else {
+        krev = blockIdx.x & ((1ull << lg_pre) - 1);
+        p0 = (uint64_t)(blockIdx.x >> lg_pre) << LG_P;
+    }
     const uint32_t np = (uint32_t)min((uint64_t)P, a.batches - p0);
     const uint64_t mask1 = (1ull << a.l_first) - 1;
     const uint64_t kpos = ((krev & mask1) << (lg_pre - a.l_first)) | (krev >> a.l_first);
@@ -732,66 +740,6 @@ __global__ void __launch_bounds__(256) transpose_rev_kernel(uint64_t *__restrict
         const uint64_t k = k0 + kl;
         const uint64_t r = lg_n ? (__brevll(k) >> (64 - lg_n)) : 0;
         out[r * batches + b0 + bl] = tile[kl * pitch + bl];
-    }
-}
-
-// The bit-reversing transpose with runs of whole leaf rows.  Split k into
-// (a | m | c) with a the top TR_LGA bits and c the low TR_LGC bits; then
-// rev(k) = (rev c | rev m | rev a), so for one m the A = 2^TR_LGA values of a
-// land on A consecutive leaf rows for every c.  A block takes one m and a
-// chunk of polynomials: it reads A runs of C = 2^TR_LGC contiguous words per
-// polynomial (16-byte loads) and writes C runs of A whole consecutive leaf
-// rows, so where the chunk holds every polynomial each run is A * batches
-// contiguous words.  Row boundaries, where 135-word rows share 32-byte
-// sectors with rows that other blocks write, come once per A rows instead of
-// once per row.  Shared tile: row (c * (A + 1) + rev a) of pitch (nb | 1);
-// the extra row per c keeps the 16-byte load side at 4 wavefronts a warp.
-#ifndef ZK_TR_LGA
-#define ZK_TR_LGA 3
-#endif
-#ifndef ZK_TR_LGC
-#define ZK_TR_LGC 4
-#endif
-#ifndef ZK_TR_THREADS
-#define ZK_TR_THREADS 512
-#endif
-constexpr uint32_t kTrA = 1u << ZK_TR_LGA, kTrC = 1u << ZK_TR_LGC;
-static_assert(ZK_TR_LGA >= 1 && ZK_TR_LGC >= 1, "row runs and 16-byte loads need A, C >= 2");
-static_assert(kTrC * (kTrA + 1) * (kTrMaxPolys | 1) * 8 <= 232448, "tile exceeds shared memory");
-constexpr size_t tr_tile_smem(uint32_t nb) { return (size_t)kTrC * (kTrA + 1) * (nb | 1) * sizeof(uint64_t); }
-
-__global__ void __launch_bounds__(ZK_TR_THREADS) transpose_rev_rows_kernel(uint64_t *__restrict__ out,
-                                                                       const uint64_t *__restrict__ in,
-                                                                       uint32_t lg_n, uint32_t batches, uint32_t chunk) {
-    extern __shared__ uint64_t tile[];
-    constexpr uint32_t A = kTrA, C = kTrC, H = C / 2, LGH = ZK_TR_LGC - 1;
-    const uint64_t N = 1ull << lg_n;
-    const uint32_t m = blockIdx.x;
-    const uint32_t mid = lg_n - ZK_TR_LGA - ZK_TR_LGC;
-    const uint32_t b0 = blockIdx.y * chunk;
-    const uint32_t nb = min(chunk, batches - b0);
-    const uint32_t pitch = nb | 1;
-    const uint64_t *src = in + (uint64_t)b0 * N + ((uint64_t)m << ZK_TR_LGC);
-#pragma unroll 4
-    for (uint32_t idx = threadIdx.x; idx < nb * A * H; idx += ZK_TR_THREADS) {
-        const uint32_t cp = idx & (H - 1), a = (idx >> LGH) & (A - 1), bl = idx >> (LGH + ZK_TR_LGA);
-        const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(src + (uint64_t)bl * N +
-                                                                    ((uint64_t)a << (lg_n - ZK_TR_LGA)) + 2 * cp);
-        const uint32_t ra = __brev(a) >> (32 - ZK_TR_LGA);
-        tile[((2 * cp) * (A + 1) + ra) * pitch + bl] = v.x;
-        tile[((2 * cp + 1) * (A + 1) + ra) * pitch + bl] = v.y;
-    }
-    __syncthreads();
-    const uint64_t rm = mid ? (uint64_t)(__brev(m) >> (32 - mid)) << ZK_TR_LGA : 0;
-    const uint32_t run = A * nb;
-    // f / run and r / nb as (x * ceil(2^32 / d)) >> 32: exact for x < 2^32 / d (here x < 2^15, d < 2^11).
-    const uint64_t inv_run = ((1ull << 32) + run - 1) / run, inv_nb = ((1ull << 32) + nb - 1) / nb;
-#pragma unroll 4
-    for (uint32_t f = threadIdx.x; f < C * run; f += ZK_TR_THREADS) {
-        const uint32_t c = (uint32_t)((f * inv_run) >> 32), r = f - c * run;
-        const uint32_t i = (uint32_t)((r * inv_nb) >> 32), bl = r - i * nb;
-        const uint64_t row = ((uint64_t)(__brev(c) >> (32 - ZK_TR_LGC)) << (lg_n - ZK_TR_LGC)) | rm | i;
-        out[row * batches + b0 + bl] = tile[(c * (A + 1) + i) * pitch + bl];
     }
 }
 
@@ -1162,9 +1110,12 @@ uint64_t ntt_leaves_scratch_elems(uint32_t lg, uint64_t batches) {
 void transpose_rev_run(uint64_t *out, const uint64_t *in, uint32_t lg_n, uint32_t batches, cudaStream_t s) {
     if (batches == 0) return;
     const uint64_t N = 1ull << lg_n;
+    const uint64_t K = std::min<uint64_t>(N, kTrK);
     const uint32_t nchunks = (batches + kTrMaxPolys - 1) / kTrMaxPolys;
     const uint32_t chunk = (batches + nchunks - 1) / nchunks;  // balanced chunks
-    require(nchunks < 65536, "transpose too large");
+    const uint64_t gx = N / K;
+    require(gx < (1ull << 31) && nchunks < 65536, "transpose too large");
+    const size_t smem = (size_t)K * (chunk | 1) * sizeof(uint64_t);
     // 16-byte loads need a 16-byte aligned input (caller pointers may be 8-byte aligned only).
     const bool vec = ((uintptr_t)in & 15) == 0;
     static std::atomic<uint64_t> attr_set{0};  // one bit per device
@@ -1173,21 +1124,8 @@ void transpose_rev_run(uint64_t *out, const uint64_t *in, uint32_t lg_n, uint32_
         const int big = (int)(kTrK * (kTrMaxPolys | 1) * sizeof(uint64_t));
         ZK_CUDA(cudaFuncSetAttribute(transpose_rev_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
         ZK_CUDA(cudaFuncSetAttribute(transpose_rev_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-        ZK_CUDA(cudaFuncSetAttribute(transpose_rev_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)tr_tile_smem(kTrMaxPolys)));
         attr_set.fetch_or(1ull << dev);
     }
-    if (vec && lg_n >= ZK_TR_LGA + ZK_TR_LGC && lg_n - ZK_TR_LGA - ZK_TR_LGC <= 31) {
-        const uint64_t gx = N >> (ZK_TR_LGA + ZK_TR_LGC);
-        transpose_rev_rows_kernel<<<dim3((unsigned)gx, nchunks), ZK_TR_THREADS, tr_tile_smem(chunk), s>>>(
-            out, in, lg_n, batches, chunk);
-        ZK_CHECK_LAUNCH();
-        return;
-    }
-    const uint64_t K = std::min<uint64_t>(N, kTrK);
-    const uint64_t gx = N / K;
-    require(gx < (1ull << 31), "transpose too large");
-    const size_t smem = (size_t)K * (chunk | 1) * sizeof(uint64_t);
     if (vec) transpose_rev_kernel<true><<<dim3((unsigned)gx, nchunks), 256, smem, s>>>(out, in, lg_n, batches, chunk);
     else transpose_rev_kernel<false><<<dim3((unsigned)gx, nchunks), 256, smem, s>>>(out, in, lg_n, batches, chunk);
     ZK_CHECK_LAUNCH();
