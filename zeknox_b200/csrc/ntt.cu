@@ -159,27 +159,13 @@ __device__ __forceinline__ void smem_dif(uint64_t *sm, const uint64_t *tw, uint3
     }
 }
 
-// Row permutation of the swizzled shared-memory layout (SWZ below): row r is
-// stored at r ^ swz_f(r), swz_f(r) = parity of bits 3, 7 and 8 of r, with a
-// pitch of exactly T words.  With 8 lines of 512 points per block, the two
-// rows that a half-warp touches in every phase of the column pass (staging,
-// zero-extension replication, each radix-8 step, the store phase's
-// bit-reversed reads) then differ in their lowest stored bit, so they fall on
-// the two halves of the banks: 2 wavefronts per 64-bit warp access instead
-// of 4 with the padded pitch.  swz_f is linear over XOR, and every access
-// below splits its row into bit fields that do not overlap (a thread's part
-// and a compile-time part), so each access picks one of two base pointers
-// per unit instead of recomputing the permutation.
-__host__ __device__ constexpr uint32_t swz_f(uint32_t r) { return ((r >> 3) ^ (r >> 7) ^ (r >> 8)) & 1u; }
-
 // smem_dif with the line length (2^LG_L), the lines per block (2^LG_T), the
 // first half-span (S) and the direction fixed at compile time: the unit loops
 // unroll and every index but the thread's own folds to a constant.  Same
-// steps and synchronisation as smem_dif.  SWZ: rows stored permuted (swz_f),
-// pitch T.
-template <int LG_L, int LG_T, int S, bool INV, bool SWZ = false>
+// steps and synchronisation as smem_dif.
+template <int LG_L, int LG_T, int S, bool INV>
 __device__ __forceinline__ void smem_dif_fixed(uint64_t *sm, const uint64_t *tw) {
-    constexpr uint32_t T = 1u << LG_T, TP = SWZ ? T : (T > 1 ? T + 1 : 1);
+    constexpr uint32_t T = 1u << LG_T, TP = T > 1 ? T + 1 : 1;
     if constexpr (S >= 2) {
         constexpr uint32_t LQ = S - 2, Q = 1u << LQ, SH8 = LG_L - 1 - S;
         constexpr uint32_t UNITS = T << (LG_L - 3);
@@ -190,27 +176,10 @@ __device__ __forceinline__ void smem_dif_fixed(uint64_t *sm, const uint64_t *tw)
             if (UNITS % kNttThreads == 0 || u < UNITS) {
                 const uint32_t t = u & (T - 1), w = u >> LG_T;
                 const uint32_t o = w & (Q - 1), e0 = ((w >> LQ) << (LQ + 3)) + o;
-                // element k of the unit is row e0 + k Q; pa[k] points at it
-                uint64_t *pa[8];
-                if constexpr (!SWZ) {
-#pragma unroll
-                    for (int k = 0; k < 8; k++) pa[k] = sm + e0 * TP + t + k * Q * TP;
-                } else if constexpr (LQ >= 1) {
-                    // e0 and k Q occupy disjoint bits: the stored row is (e0 ^ g ^ swz_f(k Q)) + k Q
-                    const uint32_t g = swz_f(e0);
-                    uint64_t *A = sm + (e0 ^ g) * TP + t, *B = sm + (e0 ^ g ^ 1u) * TP + t;
-#pragma unroll
-                    for (int k = 0; k < 8; k++) pa[k] = (swz_f(k * Q) ? B : A) + k * Q * TP;
-                } else {
-                    // Q = 1: e0 is a multiple of 8, swz_f(e0 + k) = g, stored row e0 + (k ^ g)
-                    const uint32_t g = swz_f(e0);
-                    uint64_t *PE = sm + (e0 + g) * TP + t, *PO = sm + (e0 - g) * TP + t;
-#pragma unroll
-                    for (int k = 0; k < 8; k++) pa[k] = ((k & 1) ? PO : PE) + k * TP;
-                }
+                uint64_t *b = sm + e0 * TP + t;
                 uint64_t x[8];
 #pragma unroll
-                for (int k = 0; k < 8; k++) x[k] = *pa[k];
+                for (int k = 0; k < 8; k++) x[k] = b[k * Q * TP];
                 dft8(x, INV);
                 if constexpr (LQ > 0) {
                     if (o != 0) {
@@ -220,10 +189,10 @@ __device__ __forceinline__ void smem_dif_fixed(uint64_t *sm, const uint64_t *tw)
                     }
                 }
 #pragma unroll
-                for (int k = 0; k < 8; k++) *pa[k] = x[k];
+                for (int k = 0; k < 8; k++) b[k * Q * TP] = x[k];
             }
         }
-        smem_dif_fixed<LG_L, LG_T, S - 3, INV, SWZ>(sm, tw);
+        smem_dif_fixed<LG_L, LG_T, S - 3, INV>(sm, tw);
     } else {
         __syncthreads();
         if constexpr (S == 1) {  // spans 2 and 1: radix-4 units
@@ -232,17 +201,14 @@ __device__ __forceinline__ void smem_dif_fixed(uint64_t *sm, const uint64_t *tw)
             for (uint32_t it = 0; it < (UNITS + kNttThreads - 1) / kNttThreads; it++) {
                 const uint32_t u = threadIdx.x + it * kNttThreads;
                 if (UNITS % kNttThreads == 0 || u < UNITS) {
-                    const uint32_t r0 = (u >> LG_T) << 2, t = u & (T - 1);
-                    // rows r0 .. r0 + 3 share swz_f (bits 0 and 1 do not enter it)
-                    const uint32_t g = SWZ ? swz_f(r0) : 0u;
-                    uint64_t *PE = sm + (r0 + g) * TP + t, *PO = sm + (r0 - g) * TP + t;
-                    const uint64_t x0 = PE[0], x1 = PO[TP], x2 = PE[2 * TP], x3 = PO[3 * TP];
+                    uint64_t *b = sm + ((u >> LG_T) << 2) * TP + (u & (T - 1));
+                    const uint64_t x0 = b[0], x1 = b[TP], x2 = b[2 * TP], x3 = b[3 * TP];
                     const uint64_t a0 = nt_add(x0, x2), a2 = nt_sub(x0, x2), a1 = nt_add(x1, x3);
                     const uint64_t a3 = INV ? gl_mul2_48(nt_sub(x3, x1)) : gl_mul2_48(nt_sub(x1, x3));
-                    PE[0] = nt_add(a0, a1);
-                    PO[TP] = nt_sub(a0, a1);
-                    PE[2 * TP] = nt_add(a2, a3);
-                    PO[3 * TP] = nt_sub(a2, a3);
+                    b[0] = nt_add(a0, a1);
+                    b[TP] = nt_sub(a0, a1);
+                    b[2 * TP] = nt_add(a2, a3);
+                    b[3 * TP] = nt_sub(a2, a3);
                 }
             }
             __syncthreads();
@@ -252,13 +218,11 @@ __device__ __forceinline__ void smem_dif_fixed(uint64_t *sm, const uint64_t *tw)
             for (uint32_t it = 0; it < (UNITS + kNttThreads - 1) / kNttThreads; it++) {
                 const uint32_t u = threadIdx.x + it * kNttThreads;
                 if (UNITS % kNttThreads == 0 || u < UNITS) {
-                    const uint32_t r0 = (u >> LG_T) << 1, t = u & (T - 1);
-                    const uint32_t g = SWZ ? swz_f(r0) : 0u;
-                    uint64_t *PE = sm + (r0 + g) * TP + t, *PO = sm + (r0 - g) * TP + t;
-                    uint64_t x0 = PE[0], x1 = PO[TP];
+                    uint64_t *b = sm + ((u >> LG_T) << 1) * TP + (u & (T - 1));
+                    uint64_t x0 = b[0], x1 = b[TP];
                     bfly1(x0, x1);
-                    PE[0] = x0;
-                    PO[TP] = x1;
+                    b[0] = x0;
+                    b[TP] = x1;
                 }
             }
             __syncthreads();
@@ -482,9 +446,7 @@ using PassKernel = void (*)(PassArgs);
 // constants.
 template <int LG_L, int LG_T, int LV, bool INV>
 __global__ void __launch_bounds__(kNttThreads) ntt_column_fixed(PassArgs a) {
-    // 8 lines of 512 points: the swizzled layout (swz_f), whose every phase is free of bank conflicts
-    constexpr bool SWZ = LG_L == 9 && LG_T == 3;
-    constexpr uint32_t L = 1u << LG_L, T = 1u << LG_T, TP = SWZ ? T : (T > 1 ? T + 1 : 1), RR = LG_L - LV;
+    constexpr uint32_t L = 1u << LG_L, T = 1u << LG_T, TP = T > 1 ? T + 1 : 1, RR = LG_L - LV;
     static_assert(RR == 0 || RR >= 2, "a one-stage zero extension takes the generic pass");
     static_assert(T <= kNttThreads && (T << LG_L) % kNttThreads == 0, "block elements: a multiple of the threads");
     extern __shared__ uint64_t smem[];
@@ -510,24 +472,14 @@ __global__ void __launch_bounds__(kNttThreads) ntt_column_fixed(PassArgs a) {
         // inputs (line block 1) and coset powers (line block 2) staged with asynchronous copies;
         // each thread reads back only the slots it staged, before its replication overwrites them
         constexpr uint32_t NE = (T << LV) < kNttThreads ? 1 : (T << LV) / kNttThreads;
-        // Line element e (< 2^LV) of block b sits in row (b << LV) + e; with SWZ that row is
-        // stored at (b << LV) + (e ^ swz_f(e) ^ swz_f(b << LV)), so E[swz_f(b << LV)] + (b << LV) TP.
-        auto rows_of = [&](uint32_t e, uint64_t *E[2]) {
-            const uint32_t f = SWZ ? swz_f(e) : 0u;
-            E[0] = sm + (e ^ f) * TP + t;
-            E[1] = SWZ ? sm + (e ^ f ^ 1u) * TP + t : E[0];
-        };
-        constexpr uint32_t F1 = SWZ ? swz_f(1u << LV) : 0u, F2 = SWZ ? swz_f(2u << LV) : 0u;
         if ((T << LV) >= kNttThreads || threadIdx.x < (T << LV)) {
 #pragma unroll
             for (uint32_t j = 0; j < NE; j++) {
                 const uint32_t e = e0 + j * DE;
                 const uint64_t i = i0 + ((uint64_t)e << lg_s);
                 if (i < a.n_valid) {
-                    uint64_t *E[2];
-                    rows_of(e, E);
-                    cp_async8(E[F1] + (1u << LV) * TP, src + ((uint64_t)e << lg_s));
-                    if (pre) cp_async8(E[F2] + (2u << LV) * TP, pre + i);
+                    cp_async8(&sm[((1u << LV) + e) * TP + t], src + ((uint64_t)e << lg_s));
+                    if (pre) cp_async8(&sm[((2u << LV) + e) * TP + t], pre + i);
                 }
             }
         }
@@ -537,23 +489,18 @@ __global__ void __launch_bounds__(kNttThreads) ntt_column_fixed(PassArgs a) {
             for (uint32_t j = 0; j < NE; j++) {
                 const uint32_t e = e0 + j * DE;
                 const uint64_t i = i0 + ((uint64_t)e << lg_s);
-                uint64_t *E[2];
-                rows_of(e, E);
                 uint64_t v = 0;
                 if (i < a.n_valid) {
-                    v = nt_canon(E[F1][(1u << LV) * TP]);
-                    if (pre) v = nt_mul(v, E[F2][(2u << LV) * TP]);
+                    v = nt_canon(sm[((1u << LV) + e) * TP + t]);
+                    if (pre) v = nt_mul(v, sm[((2u << LV) + e) * TP + t]);
                 }
-                E[0][0] = v;
+                sm[e * TP + t] = v;
 #pragma unroll
                 for (uint32_t b = 1; b < (1u << RR); b++)
-                    E[SWZ ? swz_f(b << LV) : 0u][(b << LV) * TP] = nt_mul(v, tw[(e * brev_const(b, RR)) & (L - 1)]);
+                    sm[((b << LV) + e) * TP + t] = nt_mul(v, tw[(e * brev_const(b, RR)) & (L - 1)]);
             }
         }
     } else {
-        // row e = e0 + j DE: e0 < DE and j DE occupy disjoint bits
-        const uint32_t f0 = SWZ ? swz_f(e0) : 0u;
-        uint64_t *E0 = sm + (e0 ^ f0) * TP + t, *E1 = SWZ ? sm + (e0 ^ f0 ^ 1u) * TP + t : E0;
 #pragma unroll
         for (uint32_t j = 0; j < (T << LG_L) / kNttThreads; j++) {
             const uint32_t e = e0 + j * DE;
@@ -563,10 +510,10 @@ __global__ void __launch_bounds__(kNttThreads) ntt_column_fixed(PassArgs a) {
                 v = nt_canon(src[(uint64_t)e << lg_s]);
                 if (pre) v = nt_mul(v, __ldg(pre + i));
             }
-            ((SWZ && swz_f(j * DE)) ? E1 : E0)[j * DE * TP] = v;
+            sm[e * TP + t] = v;
         }
     }
-    smem_dif_fixed<LG_L, LG_T, (int)LV - 1, INV, SWZ>(sm, tw);
+    smem_dif_fixed<LG_L, LG_T, (int)LV - 1, INV>(sm, tw);
     // store with the inter-pass twiddle w_N^(r k Q), one table load each (the
     // table has N <= 2^20 entries, so exponents wrap mod 2^32 harmlessly)
     const uint32_t nmask = (uint32_t)((1ull << a.lg_n) - 1);
@@ -574,17 +521,12 @@ __global__ void __launch_bounds__(kNttThreads) ntt_column_fixed(PassArgs a) {
     const uint32_t rk0 = (uint32_t)r * e0, rdk = (uint32_t)r * DE;
     const uint32_t lg_pre = a.lg_pre;
     const uint64_t *twf = a.tw_full;
-    // row kr = krt | c (krt from e0, c = rev(m DE) below DE's reversed bits): with SWZ stored at
-    // krt + (c ^ swz_f(c) ^ gs), gs = swz_f(krt), that is SE or SO (by the parity of c ^ swz_f(c)) + that value
-    const uint32_t gs = SWZ ? swz_f(krt) : 0u;
-    const uint64_t *SE = sm + (krt + gs) * TP + t, *SO = sm + (krt - gs) * TP + t;
 #pragma unroll
     for (uint32_t m = 0; m < (T << LG_L) / kNttThreads; m++) {
         const uint32_t k = e0 + m * DE;
-        const uint32_t c = brev_const(m * DE, LG_L);
-        const uint32_t cs = SWZ ? (c ^ swz_f(c)) : c;
+        const uint32_t kr = krt | brev_const(m * DE, LG_L);
         const uint64_t tw_k = __ldg(twf + (((rk0 + m * rdk) << lg_pre) & nmask));
-        dst[(uint64_t)k << lg_s] = nt_mul(((cs & 1u) ? SO : SE)[cs * TP], tw_k);
+        dst[(uint64_t)k << lg_s] = nt_mul(sm[kr * TP + t], tw_k);
     }
 }
 
