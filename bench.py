@@ -53,12 +53,20 @@ OTHER_BOUND = {1: "ALU pipe (logic of keccak-f on 32-bit halves; 99 % in ncu)",
 PROFILE_FIGURES = ROOT / "profiles" / "ncu_figures.json"
 
 
+# Host-only orchestration of the batched and served forms: the commit path whose
+# kernels the figures describe (zk_lde_leaves_async / zk_lde_async,
+# zk_transpose_rev_async, zk_merkle_async) does not run it.
+NOT_ON_THE_PROFILED_PATH = {"serve.cu", "admission.h"}
+
+
 def kernel_sources_sha256() -> str:
+    """SHA-256 over the sources that the profiled path's kernels and their launches are built from:
+    every zeknox_b200/csrc/*.cu, *.cuh and *.h but NOT_ON_THE_PROFILED_PATH."""
     import hashlib
 
     h = hashlib.sha256()
     for f in sorted((ROOT / "zeknox_b200" / "csrc").glob("*")):
-        if f.suffix in (".cu", ".cuh", ".h"):
+        if f.suffix in (".cu", ".cuh", ".h") and f.name not in NOT_ON_THE_PROFILED_PATH:
             h.update(f.name.encode())
             h.update(f.read_bytes())
     return h.hexdigest()
@@ -115,6 +123,7 @@ def write_profile_figures(csv_path, out=None) -> dict:
     inst = lambda ks: sum(k["smsp__inst_executed.sum"] for k in ks)  # noqa: E731
     names = lambda ks: [k["name"].split("(")[0][-60:] for k in ks]  # noqa: E731
     fig = {"sources_sha256": kernel_sources_sha256(),
+           "sources_note": "hash over zeknox_b200/csrc/*.cu, *.cuh, *.h except " + ", ".join(sorted(NOT_ON_THE_PROFILED_PATH)),
            "command": FIGURES_COMMAND + "; then python bench.py --figures-from figures.csv",
            "kernels": {
                f"merkle poseidon {n_pts}x{b} cap 4": {

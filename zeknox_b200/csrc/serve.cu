@@ -50,6 +50,7 @@
 #include <vector>
 
 #include "../../include/zeknox.h"
+#include "admission.h"
 #include "merkle.cuh"
 #include "ntt.cuh"
 #include "runtime.cuh"
@@ -417,45 +418,27 @@ void ZkServer::run() {
             }
         }
         if (queue.empty()) continue;
-        // Budget admission (see the header): the candidate at queue position q
-        // would delay the running jobs and the queued jobs before it; it may
-        // start if its estimate fits in each of their budgets (the oldest job,
-        // with nothing running, always may), and if it fits the HBM budget
-        // next to the memory the oldest queued job is waiting for.  Among
-        // those the shortest goes first.
+        // Budget admission (admission.h): FIFO, except that a shorter job may start
+        // ahead of or beside the jobs whose delay budgets its estimate fits in.
         std::vector<uint64_t> order(queue.begin(), queue.end());  // the queue is kept in submission order
-        uint64_t reserve = 0;
-        {
-            const Job &H = *jobs[order.front()];
-            if (in_use + H.bytes + H.run_bytes > budget) reserve = H.bytes + H.run_bytes;
-        }
-        double room = 1e300;  // smallest budget among the jobs a candidate would delay
-        for (uint64_t r : running) room = std::min(room, jobs[r]->budget_s);
-        auto pick = queue.end();
-        size_t pick_q = 0;
-        double best = 1e300;
+        std::vector<AdmitJob> aq(order.size());
         for (size_t q = 0; q < order.size(); q++) {
             const Job &J = *jobs[order[q]];
-            const uint64_t need = J.bytes + J.run_bytes + (q == 0 ? 0 : reserve);
-            if (J.est_s <= room && in_use + need <= budget && J.est_s < best) {
-                best = J.est_s;
-                pick = queue.begin() + q;
-                pick_q = q;
-            }
-            room = std::min(room, J.budget_s);
+            aq[q] = AdmitJob{J.est_s, J.budget_s, J.bytes + J.run_bytes};
         }
-        if (pick == queue.end()) {  // nothing can go until a job completes or memory is released
+        std::vector<double> rb(running.size());
+        for (size_t i = 0; i < running.size(); i++) rb[i] = jobs[running[i]]->budget_s;
+        const long pq = admission_pick(aq, rb, in_use, budget);
+        if (pq < 0) {  // nothing can go until a job completes or memory is released
             cv.wait(lk);
             continue;
         }
-        {
-            const Job &P = *jobs[*pick];
-            if (pick_q > 0 || !running.empty()) ahead++;
-            for (uint64_t r : running) jobs[r]->budget_s -= P.est_s;
-            for (size_t q = 0; q < pick_q; q++) jobs[order[q]]->budget_s -= P.est_s;
-        }
-        const uint64_t t = *pick;
-        queue.erase(pick);
+        if (pq > 0 || !running.empty()) ahead++;
+        admission_charge(aq, rb, pq);
+        for (size_t i = 0; i < running.size(); i++) jobs[running[i]]->budget_s = rb[i];
+        for (long q = 0; q < pq; q++) jobs[order[(size_t)q]]->budget_s = aq[(size_t)q].budget_s;
+        const uint64_t t = order[(size_t)pq];
+        queue.erase(queue.begin() + pq);
         Job &J = *jobs[t];
         const int s = (int)(std::find(slot_busy.begin(), slot_busy.end(), false) - slot_busy.begin());
         slot_busy[s] = true;
