@@ -250,7 +250,9 @@ ZK_EXTERN RustError zk_autotune_reset(void);
  * zk_server_wait_any returns, in completion order, each job that has finished
  * (or failed) since the last call, once; *ticket = 0 when nothing is pending or
  * when timeout_ms passes first (UINT32_MAX waits without limit).  The server
- * reserves hbm_budget_bytes in the device's memory pool when it is created. */
+ * keeps its own memory pool and reserves hbm_budget_bytes (plus an eighth for
+ * fragmentation) in it when it is created; each slot's worker thread
+ * allocates and launches the jobs admitted to it. */
 typedef struct ZkServer ZkServer;
 typedef struct {
     uint64_t completed, queued, max_queue;
